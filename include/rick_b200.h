@@ -1,0 +1,176 @@
+/*
+ * rick_b200.h -- C ABI of librick_b200.so, a B200 (sm_100a) implementation of
+ * RICK's imaging hot path: convolutional w-stacking gridding, per-w-plane 2-D
+ * inverse FFT, and the w-term phase correction summed into the dirty image.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in replacements, ABI-identical to the reference's C prototypes:
+ *       wstack            replaces w-stacking.h:39-57  (CPU/CUDA wstack)
+ *       phase_correction  replaces w-stacking.h:70-83
+ *     plus rick_fft_planes, which does the arithmetic of fftw_data
+ *     (fourier_transform.c:13-93) on explicit buffers.  They take host
+ *     pointers, accumulate into the output (the CPU path's semantics,
+ *     w-stacking.cu:530-532 and phase_correction.cu:233-235) and return void,
+ *     like the originals; rick_last_status() reports the outcome.  The
+ *     gridding kernel and PHASE_ON, compile-time macros in the reference
+ *     (Makefile:56-70), are run-time settings here: rick_set_kernel(),
+ *     rick_set_phase_on(), or the RICK_KERNEL / RICK_PHASE_ON environment
+ *     variables read on first use.
+ *
+ *  2. A status-returning plan API for device-resident pipelines: rows live in
+ *     HBM, the binned rows, the w-plane cube and cuFFT plans stay allocated
+ *     across calls, and every call is asynchronous on the caller's stream.
+ *
+ * All sizes are plain C types; no CUDA or torch type appears in a signature
+ * (streams are passed as void*, meaning cudaStream_t; NULL is the legacy
+ * default stream).  Status codes keep errcodes.h:2-6 and add new ones.
+ */
+#ifndef RICK_B200_H
+#define RICK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define RICK_OK                       0
+#define RICK_ERR_NO_THREADS_SUPPORT   1   /* errcodes.h:2 */
+#define RICK_ERR_IN_PARAMFILE         2   /* errcodes.h:3 */
+#define RICK_ERR_NOT_ENOUGH_MEM       3   /* errcodes.h:4 NOT_ENOUGH_MEM_STACKING */
+#define RICK_ERR_REDUCE               4   /* errcodes.h:5 */
+#define RICK_ERR_INVALID_ARG         16
+#define RICK_ERR_CUDA                17
+#define RICK_ERR_CUFFT               18
+#define RICK_ERR_IO                  19
+#define RICK_ERR_UNSUPPORTED         20
+#define RICK_ERR_BUDGET              21   /* serving: job does not fit the HBM budget */
+#define RICK_ERR_CANCELLED           22
+#define RICK_ERR_NO_ACCELERATORS_FOUND 255 /* errcodes.h:6 */
+
+/* ---- gridding kernels (Makefile:63-70 macros) and precision forms -------- */
+#define RICK_KERNEL_GAUSS               0  /* -DGAUSS */
+#define RICK_KERNEL_GAUSS_HI_PRECISION  1  /* -DGAUSS_HI_PRECISION */
+#define RICK_KERNEL_KAISER_BESSEL       2  /* -DKAISERBESSEL (the Makefile default) */
+
+#define RICK_PREC_FP64   0  /* "plain": FP64 grid and Z2Z FFT */
+#define RICK_PREC_MIXED  1  /* FP32 grid with FP64 tile sums, C2C FFT, FP64 w-phase */
+
+/* ---- 1. drop-in entry points -------------------------------------------- */
+
+/* w-stacking.h:39-57.  Grids num_points rows onto the w-stacked cube
+ * grid[2*num_w_planes*grid_size_y*grid_size_x] (interleaved re,im; index
+ * 2*(j + k*grid_size_x + w*grid_size_x*grid_size_y)) and ADDS to it.
+ * uu,vv,ww are normalised to [0,1]; dx = 1/grid_size_x, dw = 1/num_w_planes
+ * (init.c:11-12).  vis_* hold num_points*freq_per_chan*polarizations floats
+ * [row][chan][pol]; weight holds num_points*polarizations [row][pol].
+ * Rows whose w-plane index falls outside [0,num_w_planes) are skipped
+ * (the reference writes them out of bounds).  num_threads is unused;
+ * rank selects device rank % device_count (w-stacking.cu:279-281). */
+void wstack(int num_w_planes, unsigned int num_points, unsigned int freq_per_chan,
+            unsigned int polarizations, double *uu, double *vv, double *ww, float *vis_real,
+            float *vis_img, float *weight, double dx, double dw, int w_support,
+            int grid_size_x, int grid_size_y, double *grid, int num_threads, int rank);
+
+/* w-stacking.h:70-83.  image_{real,imag}[yaxis*xaxis] += sum over planes of
+ * gridss * exp(2*pi*i*wterm*(sqrt(1-l^2-m^2)-1)) * dwnorm * sqrt(1-l^2-m^2)
+ * (phase_correction.cu:191-250), or the plain plane sum when PHASE_ON is off
+ * or num_w_planes == 1.  gridss is a host cube laid out like wstack's grid. */
+void phase_correction(double *gridss, double *image_real, double *image_imag, int xaxis,
+                      int yaxis, int num_w_planes, int xaxistot, int yaxistot,
+                      double resolution, double wmin, double wmax, int num_threads, int rank);
+
+/* The arithmetic of fftw_data (fourier_transform.c:13-93): for every w-plane,
+ * gridss = FFTW_BACKWARD(grid) / (grid_size_x*grid_size_y).  Host buffers,
+ * may alias.  Returns a status. */
+int rick_fft_planes(const double *grid, double *gridss, int num_w_planes, int grid_size_x,
+                    int grid_size_y);
+
+/* Settings for the drop-ins (compile-time macros in the reference). */
+int rick_set_kernel(int kernel);       /* RICK_KERNEL_*; default KAISER_BESSEL */
+int rick_set_phase_on(int on);         /* PHASE_ON; default on */
+int rick_set_device(int device);       /* overrides rank % device_count */
+int rick_last_status(void);            /* status of this thread's last drop-in call */
+const char *rick_status_string(int status);
+const char *rick_last_error_message(void); /* detail of this thread's last failure */
+
+/* ---- 2. plan API (device-resident) -------------------------------------- */
+
+typedef struct rick_plan rick_plan;
+
+typedef struct rick_plan_desc {
+  int grid_size_x;        /* Nx */
+  int grid_size_y;        /* Ny */
+  int num_w_planes;       /* Nw */
+  int w_support;          /* odd, 3..15 */
+  int kernel;             /* RICK_KERNEL_* */
+  int precision;          /* RICK_PREC_* */
+  int phase_on;           /* PHASE_ON */
+  int device;             /* CUDA device ordinal, -1 = current */
+  uint64_t max_rows;      /* capacity: rows per call */
+  uint32_t freq_per_chan; /* channels per row */
+  uint32_t polarizations; /* polarisations per row (1, 2 or 4 vectorise) */
+} rick_plan_desc;
+
+typedef struct rick_plan_stats {
+  uint64_t rows_in;        /* rows passed to the last gridding call */
+  uint64_t rows_gridded;   /* rows that reached the grid */
+  uint64_t rows_dropped;   /* rows outside the cube or the one-rank sector */
+  uint64_t records;        /* binned row records (rows touching k tiles count k) */
+  uint64_t work_items;     /* gridder work items (tile chunks) */
+  uint64_t device_bytes;   /* HBM held by the plan */
+} rick_plan_stats;
+
+/* Row selection applied by the gridding calls. */
+#define RICK_ROWS_ALL      0  /* wstack semantics: grid every row given */
+#define RICK_ROWS_SECTOR0  1  /* gridding() semantics for one rank: the sector-0 rows of
+                                 gridding.c:149-188 (incl. the v-halo rule) */
+
+int rick_plan_create(rick_plan **plan, const rick_plan_desc *desc);
+int rick_plan_destroy(rick_plan *plan);
+/* Bytes of HBM a plan with this description would hold (for admission). */
+int rick_plan_footprint(const rick_plan_desc *desc, uint64_t *bytes);
+
+/* Grid device-resident rows into the plan's cube (overwrites the cube). */
+int rick_plan_grid(rick_plan *plan, uint64_t nrows, const double *uu, const double *vv,
+                   const double *ww, const float *weight, const float *vis_real,
+                   const float *vis_img, int row_selection, void *stream);
+/* In-place inverse FFT of every plane of the cube (FFTW_BACKWARD sign); the
+ * 1/(Nx*Ny) scale is carried and applied by rick_plan_phase / export. */
+int rick_plan_fft(rick_plan *plan, void *stream);
+/* image = (accumulate ? image : 0) + w-corrected plane sum; device pointers,
+ * Ny*Nx doubles each.  resolution = 1/max(|uvmin|,|uvmax|) (gridding_cpu.c:78). */
+int rick_plan_phase(rick_plan *plan, double resolution, double wmin, double wmax,
+                    double *image_real, double *image_imag, int accumulate, void *stream);
+/* grid + fft + phase in one call (stream-ordered, no host synchronisation). */
+int rick_plan_image(rick_plan *plan, uint64_t nrows, const double *uu, const double *vv,
+                    const double *ww, const float *weight, const float *vis_real,
+                    const float *vis_img, int row_selection, double resolution, double wmin,
+                    double wmax, double *image_real, double *image_imag, void *stream);
+/* The same with HOST buffers: rows are copied to HBM (pinned staging,
+ * overlapped with binning), the image is copied back; synchronous. */
+int rick_plan_image_host(rick_plan *plan, uint64_t nrows, const double *uu, const double *vv,
+                         const double *ww, const float *weight, const float *vis_real,
+                         const float *vis_img, int row_selection, double resolution,
+                         double wmin, double wmax, double *image_real, double *image_imag);
+/* Copy the cube out as FP64 interleaved (wstack layout), scaled to the
+ * FFTW-normalised values when it has been transformed.  dst may be host or
+ * device memory (is_host). Adds into dst when accumulate != 0 (device dst only). */
+int rick_plan_export_cube(rick_plan *plan, double *dst, int dst_is_host, void *stream);
+/* Load an FP64 interleaved cube (host or device) into the plan, marked as
+ * already transformed and normalised (phase_correction's input). */
+int rick_plan_import_cube(rick_plan *plan, const double *src, int src_is_host, void *stream);
+int rick_plan_get_stats(rick_plan *plan, rick_plan_stats *stats); /* synchronises */
+
+/* Names of the kernels this library launches, and how many launches it has
+ * issued in this process (for launch accounting). */
+int rick_kernel_names(const char **names, int max_names);
+unsigned long long rick_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RICK_B200_H */

@@ -1,0 +1,186 @@
+// Tiled convolutional gridding onto the w-stacked cube.
+//
+// Replaces convolve_g (w-stacking.cu:104-206), which scatters every footprint
+// cell of every row with two FP64 atomics straight into HBM.  Here a persistent
+// kernel takes work items (a bounded chunk of the binned records of one
+// 32x32 tile of one w-plane), accumulates their footprints in shared memory in
+// FP64, and writes the tile once: with plain coalesced stores when the tile is
+// a single item, or with one atomic per non-zero cell when a dense tile was
+// split over several items.  The kernel weights follow w-stacking.cu:162-180:
+//   u_dist = j + 0.5 - pos_u, table index (int)(5*|u_dist + KernelLen|),
+//   weight tab[jKer]*tab[kKer] (Gaussian / Kaiser-Bessel tables), or
+//   norm*exp(-(u_dist^2+v_dist^2)*std22) (high-precision Gaussian, evaluated
+//   as norm*exp(-u^2*std22)*exp(-v^2*std22)).
+// Table indices are computed with round-to-nearest intrinsics in FP64 from the
+// exact fractional position, so they equal the reference's indices bit for bit.
+#include "rick_internal.h"
+
+namespace rick {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kPitch = kTile + 1;  // shared-memory row pitch (avoids bank conflicts)
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// LPR lanes per record (a power of two >= w_support); 32/LPR records per warp step.
+template <typename OutT, int LPR>
+__global__ void __launch_bounds__(kGridThreads)
+    k_grid_tiles(const RecF64 *__restrict__ rec, const uint32_t *__restrict__ bin_off,
+                 const uint32_t *__restrict__ item_off, uint32_t nbins, uint32_t max_chunk,
+                 Geometry g, int kernel, const double *__restrict__ table, int accumulate,
+                 uint64_t *__restrict__ counters,
+                 typename Vec2<OutT>::type *__restrict__ cube) {
+  __shared__ double s_re[kTile * kPitch];
+  __shared__ double s_im[kTile * kPitch];
+  __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
+  __shared__ uint32_t s_item, s_bin, s_first, s_nitems;
+
+  const int ntab = kIncreasePrecision * g.support;
+  for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = table[t];
+  const uint32_t total_items = item_off[nbins];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned d = lane % LPR;                 // footprint column / row handled
+  const unsigned grp_base = lane - d;            // first lane of this record's group
+  constexpr int RPW = 32 / LPR;                  // records per warp step
+  constexpr int kWarps = kGridThreads / 32;
+  const double gnorm = kStd22 / kPi;             // w-stacking.cu:256
+  const bool hi = (kernel == RICK_KERNEL_GAUSS_HI_PRECISION);
+
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t item = (uint32_t)atomicAdd((unsigned long long *)&counters[kCntItemNext], 1ull);
+      uint32_t bin = 0;
+      if (item < total_items) {
+        // last bin b with item_off[b] <= item
+        uint32_t lo = 0, hi_b = nbins;
+        while (hi_b - lo > 1) {
+          const uint32_t mid = (lo + hi_b) >> 1;
+          if (item_off[mid] <= item) lo = mid; else hi_b = mid;
+        }
+        bin = lo;
+        s_first = item_off[bin];
+        s_nitems = item_off[bin + 1] - item_off[bin];
+      }
+      s_item = item;
+      s_bin = bin;
+    }
+    for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
+      s_re[c] = 0.0;
+      s_im[c] = 0.0;
+    }
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= total_items) break;
+    const uint32_t bin = s_bin;
+    const uint32_t chunk = item - s_first;
+    const bool single = (s_nitems == 1);
+    const int tx = (int)(bin % (uint32_t)g.ntx);
+    const int ty = (int)((bin / (uint32_t)g.ntx) % (uint32_t)g.nty);
+    const int w = (int)(bin / ((uint32_t)g.ntx * (uint32_t)g.nty));
+    const int x0 = tx * kTile, y0 = ty * kTile;
+    const uint32_t r0 = bin_off[bin] + chunk * max_chunk;
+    const uint32_t r1 = min(bin_off[bin + 1], r0 + max_chunk);
+
+    // Footprints of the chunk's records into the shared tile.
+    for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
+      const uint32_t r = rb + lane / LPR;
+      const bool valid = r < r1;
+      RecF64 q;
+      if (valid) q = rec[r];
+      else { q.sre = q.sim = q.fu = q.fv = 0.0; q.gu = q.gv = -1000000; }
+      double wu = 0.0, wv = 0.0;
+      if (valid && (int)d < g.support) {
+        const double off = __dadd_rn((double)((int)d - g.half), 0.5);
+        const double ud = __dsub_rn(off, q.fu);  // == (j + 0.5) - pos_u exactly
+        const double vd = __dsub_rn(off, q.fv);
+        if (hi) {
+          wu = exp(-__dmul_rn(ud, ud) * kStd22);
+          wv = exp(-__dmul_rn(vd, vd) * kStd22);
+        } else {
+          const int jk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(ud, (double)g.half)));
+          const int kk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(vd, (double)g.half)));
+          // In range for positions >= 0; rows with u or v in (-dx, 0) would index
+          // past the table (the reference reads out of bounds there): clamp.
+          wu = s_tab[min(jk, ntab - 1)];
+          wv = s_tab[min(kk, ntab - 1)];
+        }
+      }
+      const int j = q.gu - g.half + (int)d;
+      const bool col_ok = valid && (int)d < g.support && j >= 0 && j < g.nx && j >= x0 && j < x0 + kTile;
+      const double su = hi ? gnorm * wu : wu;
+      for (int e = 0; e < g.support; e++) {
+        const double wve = __shfl_sync(kFull, wv, grp_base + e);
+        const int k = q.gv - g.half + e;
+        if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
+          const double cw = su * wve;
+          const int cell = (k - y0) * kPitch + (j - x0);
+          atomicAdd(&s_re[cell], q.sre * cw);
+          atomicAdd(&s_im[cell], q.sim * cw);
+        }
+      }
+    }
+    __syncthreads();
+
+    // Flush the tile.
+    const uint64_t plane = (uint64_t)g.nx * g.ny;
+    for (int c = threadIdx.x; c < kTile * kTile; c += blockDim.x) {
+      const int y = c / kTile, x = c % kTile;
+      const int gy = y0 + y, gx = x0 + x;
+      if (gy >= g.ny || gx >= g.nx) continue;
+      const uint64_t idx = (uint64_t)w * plane + (uint64_t)gy * g.nx + gx;
+      const double vr = s_re[y * kPitch + x], vi = s_im[y * kPitch + x];
+      if (single) {
+        if (accumulate) {
+          auto o = cube[idx];
+          o.x += (OutT)vr;
+          o.y += (OutT)vi;
+          cube[idx] = o;
+        } else {
+          typename Vec2<OutT>::type o;
+          o.x = (OutT)vr;
+          o.y = (OutT)vi;
+          cube[idx] = o;
+        }
+      } else if (vr != 0.0 || vi != 0.0) {
+        atomicAdd(&cube[idx].x, (OutT)vr);
+        atomicAdd(&cube[idx].y, (OutT)vi);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename OutT>
+int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accumulate,
+                uint32_t max_chunk, cudaStream_t st) {
+  const int sms = num_sms();
+  using V = typename Vec2<OutT>::type;
+  const uint32_t nbins = (uint32_t)g.nbins();
+  // 16 KB + 16 KB of tile: several blocks per SM
+  const int blocks = sms * 6;
+  RICK_LAUNCHED();
+  if (g.support <= 8)
+    k_grid_tiles<OutT, 8><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
+                                                           nbins, max_chunk, g, kernel, s.table,
+                                                           accumulate, s.counters, (V *)cube);
+  else
+    k_grid_tiles<OutT, 16><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
+                                                            nbins, max_chunk, g, kernel, s.table,
+                                                            accumulate, s.counters, (V *)cube);
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
+}  // namespace
+
+int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
+               int accumulate, uint32_t max_chunk, cudaStream_t st) {
+  if (precision == RICK_PREC_FP64) return launch_grid<double>(g, kernel, s, cube, accumulate, max_chunk, st);
+  return launch_grid<float>(g, kernel, s, cube, accumulate, max_chunk, st);
+}
+
+}  // namespace rick

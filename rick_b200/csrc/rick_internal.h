@@ -1,0 +1,120 @@
+// Internal declarations shared by the librick_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "rick_b200.h"
+
+namespace rick {
+
+// Truncated pi of the reference (allvars.h:47, w-stacking.h:6); the w-phase and
+// the Gaussian norm use it, and 1e-12 parity needs the same constant.
+constexpr double kPi = 3.14159265359;
+// Oversampling of the 1-D kernel tables (w-stacking.cu:253).
+constexpr int kIncreasePrecision = 5;
+// Gaussian width 1/(2 std^2) with std = 1 (w-stacking.cu:254-255).
+constexpr double kStd22 = 0.5;
+// Edge of a grid tile owned by one gridder work item.
+constexpr int kTile = 32;
+// Largest supported w_support (odd): footprints fit inside one tile border.
+constexpr int kMaxSupport = 15;
+// Threads per gridder block.
+constexpr int kGridThreads = 256;
+
+// Status plumbing: every internal call returns an int status and records a
+// message in thread-local storage.
+int set_error(int status, const char *fmt, ...);
+int cuda_status(cudaError_t e, const char *what, const char *file, int line);
+int cufft_status(cufftResult r, const char *what, const char *file, int line);
+
+#define RICK_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) return ::rick::cuda_status(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+#define RICK_CUFFT(call)                                                               \
+  do {                                                                                 \
+    cufftResult r_ = (call);                                                           \
+    if (r_ != CUFFT_SUCCESS) return ::rick::cufft_status(r_, #call, __FILE__, __LINE__); \
+  } while (0)
+#define RICK_TRY(call)            \
+  do {                            \
+    int s_ = (call);              \
+    if (s_ != RICK_OK) return s_; \
+  } while (0)
+
+// Geometry of one imaging job, as the kernels see it.
+struct Geometry {
+  int nx, ny, nw;       // grid_size_x, grid_size_y, num_w_planes
+  int support;          // w_support (odd)
+  int half;             // KernelLen = (w_support-1)/2
+  int ntx, nty;         // tiles per row / column
+  double dx, dw;        // 1/Nx, 1/Nw (init.c:11-12) or as passed to wstack
+  double w_supporth;    // (double)half*dx (init.c:13)
+  int select_sector0;   // apply gridding.c:149-188 membership
+  uint64_t nbins() const { return (uint64_t)nw * ntx * nty; }
+};
+
+// Binned row record of the FP64 form.  fu, fv are pos - (int)pos, exact in
+// FP64, so (d + 0.5) - f rounds to the reference's (j + 0.5) - pos exactly.
+struct __align__(8) RecF64 {
+  double sre, sim;   // sum over channels and polarisations of weight*vis
+  double fu, fv;     // fractional pixel position
+  int gu, gv;        // integer pixel position (truncated toward zero)
+};
+
+// Device scratch owned by a plan.
+struct Scratch {
+  uint32_t *bin_count = nullptr;   // [nbins+1] counts, then exclusive offsets
+  uint32_t *bin_cursor = nullptr;  // [nbins]
+  uint32_t *item_off = nullptr;    // [nbins+1] work-item offsets
+  uint32_t *item_bin = nullptr;    // [max_items]
+  uint32_t *heavy = nullptr;       // [nbins] bins split into several items
+  uint32_t *scan_tmp = nullptr;    // block sums for the scans
+  uint64_t *counters = nullptr;    // [8] device counters (see Counter)
+  RecF64 *records = nullptr;       // [max_records]
+  uint64_t max_records = 0;
+  uint64_t max_items = 0;
+  double *table = nullptr;         // 1-D kernel table, 5*support doubles
+};
+
+enum Counter : int {
+  kCntDropped = 0,    // rows outside the cube / sector
+  kCntGridded = 1,    // rows that produced records
+  kCntRecords = 2,    // records written
+  kCntItemNext = 3,   // persistent gridder work counter
+  kCntHeavy = 4,      // number of heavy bins
+  kCntOverflow = 5,   // records beyond capacity (must stay 0)
+  kNumCounters = 8
+};
+
+// Kernel-table construction on the host (w-stacking.cu:35-89).
+void make_table(int kernel, int support, double *tab);
+
+// Pipeline stages (bin.cu, grid.cu, phase.cu).
+int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
+             const double *vv, const double *ww, const float *weight, const float *vis_re,
+             const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
+             uint32_t max_chunk, cudaStream_t st);
+int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
+               int accumulate, uint32_t max_chunk, cudaStream_t st);
+void phase_tables(int xaxis, int yaxis, int xaxistot, int yaxistot, double resolution,
+                  double *l, double *m);
+int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, const double *ltab,
+              const double *mtab, double wmin, double wmax, double norm, int phase_on,
+              int accumulate, double *img_re, double *img_im, cudaStream_t st);
+int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *tmp,
+                       cudaStream_t st);
+uint64_t scan_tmp_words(uint64_t n);
+
+int num_sms();
+
+// Kernels launched by this library (reported by rick_launch_count).
+extern std::atomic<unsigned long long> g_launches;
+#define RICK_LAUNCHED() (::rick::g_launches++)
+
+}  // namespace rick
