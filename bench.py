@@ -1,0 +1,430 @@
+"""Benchmark: imaged visibilities/s of the imaging hot path on B200.
+
+Workload (one "step" = one imaging job: binning -> gridding -> per-plane inverse
+FFT -> w-correction + plane sum, all rows): the LOFAR-like large single image,
+60 stations log-radial to 40 km, 4 h at dec +50, 5 s integrations
+(1770 baselines x 2880 steps; 5,096,600 rows after the 1000-row drop), 64
+channels x 4 polarisations (1.305e9 visibilities), 200 log-normal point
+sources + noise sigma 0.5, grid 4096^2 x 32 w-planes, Kaiser-Bessel support 7.
+Synthetic, seeded, generated on the GPU (no dataset ships with the reference).
+
+  value     imaged vis/s with the rows resident in HBM (FP64 plain form, the
+            reference's arithmetic), CUDA events on the launching stream,
+            max over ranks; inputs (10.6 GB) are larger than L2.
+  e2e       the same through rick_plan_image_host (host buffers, pinned;
+            H2D of the rows and D2H of the image inside the timed region).
+  forms     plain FP64 and mixed (FP32 grid/FFT) side by side, with the mixed
+            image's relative L2 error against the FP64 image.
+  roofline  the dominant stage: algorithmic bytes / its CUDA-event time over
+            the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own CPU wstack + phase_correction (compiled from
+            its sources, oracle/_ref, OpenMP on all host cores) with scipy's
+            FFT (FFTW is absent), on a bounded sample, extrapolated.
+
+--impl reference prints the reference arm (the same CPU path, timed per step).
+With N GPUs (torchrun) each rank images its own copy of the job (replicas,
+weak scaling; the path needs no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "imaged vis/s (1xB200) FP32-mixed vs FP64 plain @<=1e-5 rel err; p50/p99 lat"
+WORKLOAD = dict(name="c2", grid=4096, w_planes=32, kernel="kaiser_bessel", w_support=7)
+
+# DRAM traffic per launch measured by ncu for the dominant kernels (bytes),
+# scaled to the full workload (profiles/ summaries give the captures).
+NCU_TRAFFIC = {}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--time-fraction", type=float, default=1.0,
+                    help="keep this leading fraction of the time steps (debug only)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(n_rows, nvis, npol, records, nx, ny, nw, val_bytes):
+    """Per-stage algorithmic bytes (the minimum each stage must move)."""
+    g = 2 * nw * nx * ny * val_bytes                 # the cube
+    rec = 40 * records                                # binned row records
+    return {
+        "bin_count": 24 * n_rows,                                   # u,v,w read once
+        "bin_scatter": 8 * nvis + n_rows * (24 + 4 * npol) + rec,   # vis+uvw+weights in, records out
+        "cube_zero": g,
+        "grid": rec + g,                                            # records in, cube out
+        "fft": 2 * g,                                               # one read + one write
+        "phase": g + 16 * nx * ny,                                  # cube in, FP64 image out
+    }
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import rick_b200 as R
+    from rick_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    cfg = synth.CONFIGS[WORKLOAD["name"]]
+    t0 = time.time()
+    obs = synth.make_observation(cfg, seed=2024, device=str(dev),
+                                 time_fraction=args.time_fraction)
+    torch.cuda.synchronize()
+    gen_s = time.time() - t0
+    n = R.rows_read(obs.meta)
+    nchan, npol = cfg.nchan, cfg.npol
+    nv = nchan * npol
+    rows = (obs.uu[:n].contiguous(), obs.vv[:n].contiguous(), obs.ww[:n].contiguous(),
+            obs.weights[: n * npol].contiguous(), obs.vis_re[: n * nv].contiguous(),
+            obs.vis_im[: n * nv].contiguous())
+    nvis = n * nv
+    res = R.resolution_of(obs.meta)
+    wmin, wmax = obs.meta["wmin"], obs.meta["wmax"]
+    nx = ny = cfg.grid
+    nw = cfg.w_planes
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def run_form(precision):
+        geom = R.Geometry(nx, ny, nw, cfg.w_support, cfg.kernel, precision)
+        plan = R.Plan(geom, n, nchan, npol, device=local)
+        img = torch.empty(2 * nx * ny, dtype=torch.float64, device=dev)
+        step = lambda: plan.image(n, rows, res, wmin, wmax, img[: nx * ny], img[nx * ny:],
+                                  R.ROWS_SECTOR0, stream)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = R.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = R.launch_count() - launches0
+        ms = e0.elapsed_time(e1) / args.steps
+        barrier()
+        # per-stage times (stage events on the same stream), a second pass
+        plan.set_timing(True)
+        stage = {}
+        lat = []
+        for _ in range(max(3, min(args.steps, 10))):
+            step()
+            s = plan.stage_ms()
+            lat.append(sum(s.values()))
+            for k, v in s.items():
+                stage[k] = stage.get(k, 0.0) + v
+        k = max(3, min(args.steps, 10))
+        stage = {kk: v / k for kk, v in stage.items()}
+        plan.set_timing(False)
+        stats = plan.stats()
+        image = img.clone()
+        return plan, image, ms, stage, stats, launches, lat
+
+    with ClockSampler(local) as clocks:
+        plan64, img64, ms64, stage64, stats64, launches, lat64 = run_form("fp64")
+    plan64.close()
+    planmx, imgmx, msmx, stagemx, statsmx, _, latmx = run_form("mixed")
+    err_mixed = float(torch.linalg.vector_norm(imgmx - img64) / torch.linalg.vector_norm(img64))
+    planmx.close()
+
+    # max over ranks
+    t = torch.tensor([ms64, msmx], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms64, msmx = float(t[0]), float(t[1])
+    value = world * nvis / (ms64 * 1e-3)
+
+    # ---- e2e through the host C-ABI entry point (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        host = [r.cpu().pin_memory() for r in rows]
+        h_img = torch.empty(2 * nx * ny, dtype=torch.float64).pin_memory()
+        geom = R.Geometry(nx, ny, nw, cfg.w_support, cfg.kernel, "fp64")
+        with R.Plan(geom, n, nchan, npol, device=local) as plan:
+            call = lambda: plan.image_host(n, host, res, wmin, wmax, h_img[: nx * ny],
+                                           h_img[nx * ny:], R.ROWS_SECTOR0)
+            call()
+            k_e2e = max(1, min(args.steps, 5))
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(k_e2e):
+                call()
+            e2e_s = (time.perf_counter() - t0) / k_e2e
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt[0])
+        bi = sum(int(h.numel() * h.element_size()) for h in host)
+        e2e = {"value": world * nvis / e2e_s, "unit": "vis/s", "h2d_bytes_per_step": bi,
+               "d2h_bytes_per_step": int(h_img.numel() * 8), "steps": k_e2e,
+               "ms_per_step": e2e_s * 1e3}
+        del host
+
+    hbm, peak_kind = peaks()
+    alg = algorithmic_bytes(n, nvis, npol, stats64["records"], nx, ny, nw, 8)
+    dom = max(stage64, key=stage64.get)
+    achieved = alg[dom] / (stage64[dom] * 1e-3) / 1e9
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "traffic": NCU_TRAFFIC.get(dom), "peak_source": peak_kind,
+                "algorithmic_bytes": alg[dom],
+                "stages_ms": {k: round(v, 4) for k, v in stage64.items()},
+                "stages_frac": {k: round(alg[k] / (v * 1e-3) / 1e9 / hbm, 4)
+                                for k, v in stage64.items() if v > 0}}
+    g8 = 2 * nw * nx * ny * 8
+    pipe_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(obs, n, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, steps=1)
+    line = {
+        "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "LOFAR-like single image: 5,096,600 rows x 64 chan x 4 pol "
+                               "(1.305e9 vis), 4096^2 x 32 w-planes, Kaiser-Bessel support 7",
+                   "rows": n, "visibilities": nvis, "grid": nx, "w_planes": nw,
+                   "kernel": cfg.kernel, "w_support": cfg.w_support,
+                   "l2": "inputs (10.6 GB) larger than L2; no flush",
+                   "parallelism": f"replicas x{world}", "time_fraction": args.time_fraction},
+        "e2e": e2e, "gpu_launches": launches,
+        "roofline": roofline,
+        "pipeline_roofline": {"bytes": pipe_bytes, "achieved_gbs": pipe_bytes / (ms64 * 1e-3) / 1e9,
+                              "frac": pipe_bytes / (ms64 * 1e-3) / 1e9 / hbm},
+        "forms": {"fp64": {"vis_per_s": world * nvis / (ms64 * 1e-3), "ms": ms64,
+                           "stages_ms": stage64,
+                           "p50_ms": float(np.percentile(lat64, 50)),
+                           "p99_ms": float(np.percentile(lat64, 99))},
+                  "mixed": {"vis_per_s": world * nvis / (msmx * 1e-3), "ms": msmx,
+                            "stages_ms": stagemx,
+                            "p50_ms": float(np.percentile(latmx, 50)),
+                            "p99_ms": float(np.percentile(latmx, 99)),
+                            "rel_l2_vs_fp64": err_mixed},
+                  "mixed_over_fp64": ms64 / msmx},
+        "job": {"rows_gridded": stats64["rows_gridded"], "rows_dropped": stats64["rows_dropped"],
+                "records": stats64["records"], "work_items": stats64["work_items"],
+                "generate_s": gen_s},
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        line["clocks"] = clocks.summary()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(obs, n, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, steps=1,
+                 target_s=6.0):
+    """The reference's CPU path on a bounded sample, extrapolated to the job.
+
+    wstack: the reference's own compiled CPU wstack (oracle/_ref, OpenMP, all host
+    threads) on the first S packed rows, scaled by rows/S; FFT: scipy.fft.ifft2 FP64
+    (workers = all threads; FFTW is absent) on P planes, scaled by Nw/P;
+    phase_correction: the reference's own on P planes, scaled by Nw/P.
+    Falls back to the oracle restatement ("port") where oracle/_ref is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import torch
+
+    threads = _threads()
+    kind = "reference" if O.ref_available(cfg.kernel) else "port"
+    nv = nchan * npol
+
+    def host(x, count):
+        return np.ascontiguousarray(x[:count].cpu().numpy() if hasattr(x, "cpu") else x[:count])
+
+    # a first small sample sizes the real one to about target_s of wstack
+    def time_wstack(S):
+        uu, vv, ww = host(obs.uu, S), host(obs.vv, S), host(obs.ww, S)
+        wt, vr, vi = host(obs.weights, S * npol), host(obs.vis_re, S * nv), host(obs.vis_im, S * nv)
+        keep = (ww * nw).astype(np.int64) < nw
+        uu, vv, ww = uu[keep], vv[keep], ww[keep]
+        wt = wt.reshape(-1, npol)[keep].ravel(); vr = vr.reshape(-1, nv)[keep].ravel()
+        vi = vi.reshape(-1, nv)[keep].ravel()
+        plane_grid = np.zeros(2 * nw * nx * ny)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_lib(cfg.kernel).wstack(nw, len(uu), nchan, npol, uu, vv, ww, vr, vi, wt, 1 / nx,
+                                        1 / nw, cfg.w_support, nx, ny, plane_grid, threads, 0)
+        else:
+            O.wstack(cfg.kernel, nw, nchan, npol, uu, vv, ww, vr, vi, wt, 1 / nx, 1 / nw,
+                     cfg.w_support, nx, ny, plane_grid, threads)
+        return time.perf_counter() - t0, plane_grid
+
+    S0 = min(n, 20000)
+    t_small, _ = time_wstack(S0)
+    S = int(min(n, max(S0, S0 * target_s / max(t_small, 1e-3))))
+    results = []
+    for _ in range(steps):
+        t_w, grid = time_wstack(S)
+        P = 2
+        sub = np.ascontiguousarray(grid[: 2 * P * nx * ny])
+        t0 = time.perf_counter()
+        gss = O.fft_planes(sub, P, nx, ny, workers=threads)
+        t_f = time.perf_counter() - t0
+        img_re, img_im = np.zeros(nx * ny), np.zeros(nx * ny)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_lib(cfg.kernel).phase_correction(gss, img_re, img_im, nx, ny, P, nx, ny, res,
+                                                  wmin, wmax, threads, 0)
+        else:
+            O.phase_correction(gss, nx, ny, P, res, wmin, wmax, True, threads, img_re, img_im)
+        t_p = time.perf_counter() - t0
+        est = t_w * (n / S) + (t_f + t_p) * (nw / P)
+        results.append(dict(est=est, t_w=t_w, t_f=t_f, t_p=t_p))
+    est = float(np.median([r["est"] for r in results]))
+    r0 = results[0]
+    del torch
+    return {"value": n * nv / est, "unit": "vis/s", "cores": threads, "kind": kind,
+            "sample": f"wstack on {S} of {n} rows (x{n / S:.1f}), FFT (scipy.fft, FFTW absent) "
+                      f"and phase_correction on 2 of {nw} planes (x{nw / 2:.0f}); "
+                      f"sample times wstack {r0['t_w']:.2f}s fft {r0['t_f']:.2f}s "
+                      f"phase {r0['t_p']:.2f}s",
+            "est_job_s": est}
+
+
+def run_reference(args):
+    """Reference arm: the reference's own CPU path, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import rick_b200  # noqa: F401  (synthetic generator only)
+    from rick_b200 import synth
+    import torch
+
+    cfg = synth.CONFIGS[WORKLOAD["name"]]
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    obs = synth.make_observation(cfg, seed=2024, device=dev, time_fraction=args.time_fraction)
+    import rick_b200 as R
+    n = R.rows_read(obs.meta)
+    nv = cfg.nchan * cfg.npol
+    res = R.resolution_of(obs.meta)
+    for _ in range(args.warmup):
+        pass  # the sample sizing inside cpu_baseline warms the caches
+    cpu = cpu_baseline(obs, n, cfg.nchan, cfg.npol, cfg.grid, cfg.grid, cfg.w_planes, cfg, res,
+                       obs.meta["wmin"], obs.meta["wmax"], steps=max(1, min(args.steps, 3)))
+    line = {"metric": METRIC, "value": cpu["value"], "unit": "vis/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cpu["est_job_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "LOFAR-like single image: 5,096,600 rows x 64 chan x 4 pol "
+                                   "(1.305e9 vis), 4096^2 x 32 w-planes, Kaiser-Bessel support 7",
+                       "rows": n, "visibilities": n * nv},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "vis/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

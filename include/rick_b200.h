@@ -165,6 +165,17 @@ int rick_plan_export_cube(rick_plan *plan, double *dst, int dst_is_host, void *s
 int rick_plan_import_cube(rick_plan *plan, const double *src, int src_is_host, void *stream);
 int rick_plan_get_stats(rick_plan *plan, rick_plan_stats *stats); /* synchronises */
 
+/* Stage timers (the counterpart of the reference's timing_wt stage times,
+ * timing.h:60-76): when enabled, every plan call records CUDA events around
+ * its stages on the caller's stream; rick_plan_stage_ms reports the last call's
+ * milliseconds per stage (synchronises) in the order
+ *   0 bin_count (histogram + scans), 1 bin_scatter (row sums + records),
+ *   2 cube_zero, 3 grid (tiled gridder), 4 fft, 5 phase (w-correction + sum);
+ * a stage that did not run in the last call reports -1. */
+#define RICK_NUM_STAGES 6
+int rick_plan_set_timing(rick_plan *plan, int on);
+int rick_plan_stage_ms(rick_plan *plan, float *ms, int n);
+
 /* Names of the kernels this library launches, and how many launches it has
  * issued in this process (for launch accounting). */
 int rick_kernel_names(const char **names, int max_names);

@@ -104,13 +104,16 @@ def lib():
     L.rick_plan_export_cube.argtypes = [_vp, _vp, C.c_int, _vp]
     L.rick_plan_import_cube.argtypes = [_vp, _vp, C.c_int, _vp]
     L.rick_plan_get_stats.argtypes = [_vp, C.POINTER(PlanStats)]
+    L.rick_plan_set_timing.argtypes = [_vp, C.c_int]
+    L.rick_plan_stage_ms.argtypes = [_vp, C.POINTER(C.c_float), C.c_int]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
     L.rick_launch_count.argtypes = []
     L.rick_launch_count.restype = C.c_ulonglong
     for fn in ["rick_plan_create", "rick_plan_destroy", "rick_plan_footprint", "rick_plan_grid",
                "rick_plan_fft", "rick_plan_phase", "rick_plan_image", "rick_plan_image_host",
                "rick_plan_export_cube", "rick_plan_import_cube", "rick_plan_get_stats",
-               "rick_kernel_names", "rick_fft_planes"]:
+               "rick_kernel_names", "rick_fft_planes", "rick_plan_set_timing",
+               "rick_plan_stage_ms"]:
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L
@@ -297,6 +300,16 @@ class Plan:
     def import_cube(self, src, src_is_host, stream=None):
         check(lib().rick_plan_import_cube(self._h, _ptr(src), int(src_is_host), _stream(stream)),
               "rick_plan_import_cube")
+
+    STAGES = ("bin_count", "bin_scatter", "cube_zero", "grid", "fft", "phase")
+
+    def set_timing(self, on: bool = True):
+        check(lib().rick_plan_set_timing(self._h, int(on)), "rick_plan_set_timing")
+
+    def stage_ms(self) -> dict:
+        arr = (C.c_float * len(self.STAGES))()
+        check(lib().rick_plan_stage_ms(self._h, arr, len(self.STAGES)), "rick_plan_stage_ms")
+        return {k: float(arr[i]) for i, k in enumerate(self.STAGES) if arr[i] >= 0}
 
     def stats(self) -> dict:
         s = PlanStats()

@@ -248,7 +248,7 @@ void launch_scatter(int blocks, cudaStream_t st, const double *uu, const double 
 int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
              const double *vv, const double *ww, const float *weight, const float *vis_re,
              const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
-             uint32_t max_chunk, cudaStream_t st) {
+             uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid) {
   (void)kernel;
   (void)precision;
   const uint64_t nbins = g.nbins();
@@ -256,6 +256,7 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
   RICK_CUDA(cudaMemsetAsync(s.bin_cursor, 0, nbins * sizeof(uint32_t), st));
   if (nrows == 0) {
     RICK_CUDA(cudaMemsetAsync(s.item_off, 0, (nbins + 1) * sizeof(uint32_t), st));
+    if (mid) RICK_CUDA(cudaEventRecord(mid, st));
     return RICK_OK;
   }
   const int sms = num_sms();
@@ -272,6 +273,7 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
   k_item_count<<<blocks_items, 256, 0, st>>>(s.bin_count, nbins, max_chunk, s.item_off);
   RICK_CUDA(cudaGetLastError());
   RICK_TRY(exclusive_scan_u32(s.item_off, s.item_off, nbins + 1, s.scan_tmp, st));
+  if (mid) RICK_CUDA(cudaEventRecord(mid, st));
 
   const uint64_t nv = (uint64_t)nchan * npol;
   const bool aligned = ((uintptr_t)vis_re % 16 == 0) && ((uintptr_t)vis_im % 16 == 0);

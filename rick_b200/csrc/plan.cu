@@ -138,6 +138,11 @@ struct rick_plan {
   size_t stage_bytes = 0;
   uint64_t last_rows = 0;
   size_t device_bytes = 0;
+  // stage timers: ev[k] marks the start of stage k, ev[k+1] its end
+  bool timing = false;
+  cudaEvent_t ev[RICK_NUM_STAGES + 1] = {};
+  bool ran[RICK_NUM_STAGES] = {};
+  cudaEvent_t ev_fft0 = nullptr, ev_phase0 = nullptr;
 };
 
 namespace {
@@ -260,6 +265,11 @@ struct DeviceGuard {
   }
 };
 
+int mark(rick_plan *p, cudaEvent_t e, cudaStream_t st) {
+  if (p->timing && e) RICK_CUDA(cudaEventRecord(e, st));
+  return RICK_OK;
+}
+
 int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
                    const double *ww, const float *weight, const float *vis_re, const float *vis_im,
                    int select, int accumulate, double dx, double dw, cudaStream_t st) {
@@ -269,12 +279,20 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
   if (nrows && (!uu || !vv || !ww || !weight || !vis_re || !vis_im))
     return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
   fill_geometry(p, dx, dw, select);
+  for (int k = 0; k < RICK_NUM_STAGES; k++) p->ran[k] = false;
+  RICK_TRY(mark(p, p->ev[0], st));
   RICK_CUDA(cudaMemsetAsync(p->s.counters, 0, kNumCounters * sizeof(uint64_t), st));
   const uint32_t chunk = choose_chunk(nrows);
   RICK_TRY(bin_rows(p->g, p->d.kernel, p->d.precision, nrows, uu, vv, ww, weight, vis_re, vis_im,
-                    p->d.freq_per_chan, p->d.polarizations, p->s, chunk, st));
+                    p->d.freq_per_chan, p->d.polarizations, p->s, chunk, st,
+                    p->timing ? p->ev[1] : nullptr));
+  RICK_TRY(mark(p, p->ev[2], st));
   if (!accumulate) RICK_CUDA(cudaMemsetAsync(p->cube, 0, p->cube_vals * p->val_bytes, st));
+  RICK_TRY(mark(p, p->ev[3], st));
   RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, chunk, st));
+  RICK_TRY(mark(p, p->ev[4], st));
+  p->ran[0] = p->ran[1] = p->ran[3] = true;
+  p->ran[2] = !accumulate;
   p->cube_state = kCubeRaw;
   p->last_rows = nrows;
   return RICK_OK;
@@ -285,6 +303,7 @@ int plan_fft_impl(rick_plan *p, cudaStream_t st) {
     return set_error(RICK_ERR_INVALID_ARG, "cube already transformed");
   if (!p->fft) RICK_TRY(choose_fft(p));
   RICK_CUFFT(cufftSetStream(p->fft, st));
+  RICK_TRY(mark(p, p->ev_fft0, st));
   const uint64_t plane = (uint64_t)p->d.grid_size_x * p->d.grid_size_y;
   for (int b0 = 0; b0 < p->d.num_w_planes; b0 += p->fft_batch) {
     if (p->d.precision == RICK_PREC_FP64) {
@@ -295,6 +314,8 @@ int plan_fft_impl(rick_plan *p, cudaStream_t st) {
       RICK_CUFFT(cufftExecC2C(p->fft, ptr, ptr, CUFFT_INVERSE));
     }
   }
+  RICK_TRY(mark(p, p->ev[5], st));
+  p->ran[4] = true;
   p->cube_state = kCubeTransformed;
   return RICK_OK;
 }
@@ -313,9 +334,12 @@ int plan_phase_impl(rick_plan *p, int xtot, int ytot, double resolution, double 
     return set_error(RICK_ERR_INVALID_ARG, "phase correction needs a transformed cube");
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
   RICK_TRY(ensure_lm(p, nx, ny, xtot, ytot, resolution, st));
+  RICK_TRY(mark(p, p->ev_phase0, st));
   RICK_TRY(phase_sum(p->d.precision, p->cube, nx, ny, p->d.num_w_planes, p->d_lm, p->d_lm + nx,
                      wmin, wmax, cube_scale(p), p->d.phase_on, accumulate, img_re, img_im, st));
   g_launches++;
+  RICK_TRY(mark(p, p->ev[6], st));
+  p->ran[5] = true;
   return RICK_OK;
 }
 
@@ -400,6 +424,10 @@ int rick_plan_destroy(rick_plan *p) {
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->h_lm) cudaFreeHost(p->h_lm);
+  for (cudaEvent_t e : p->ev)
+    if (e) cudaEventDestroy(e);
+  if (p->ev_fft0) cudaEventDestroy(p->ev_fft0);
+  if (p->ev_phase0) cudaEventDestroy(p->ev_phase0);
   delete p;
   return RICK_OK;
 }
@@ -622,6 +650,32 @@ int rick_internal_plan_phase_full(rick_plan *p, int xtot, int ytot, double resol
 }
 
 const rick_plan_desc *rick_internal_plan_desc(const rick_plan *p) { return &p->d; }
+
+int rick_plan_set_timing(rick_plan *p, int on) {
+  if (!p) return set_error(RICK_ERR_INVALID_ARG, "null plan");
+  DeviceGuard guard(p->device);
+  if (on && !p->ev[0]) {
+    for (cudaEvent_t &e : p->ev) RICK_CUDA(cudaEventCreate(&e));
+    RICK_CUDA(cudaEventCreate(&p->ev_fft0));
+    RICK_CUDA(cudaEventCreate(&p->ev_phase0));
+  }
+  p->timing = on != 0;
+  return RICK_OK;
+}
+
+int rick_plan_stage_ms(rick_plan *p, float *ms, int n) {
+  if (!p || !ms) return set_error(RICK_ERR_INVALID_ARG, "null argument");
+  DeviceGuard guard(p->device);
+  if (!p->ev[0]) return set_error(RICK_ERR_INVALID_ARG, "stage timing was never enabled");
+  RICK_CUDA(cudaDeviceSynchronize());
+  const cudaEvent_t start[RICK_NUM_STAGES] = {p->ev[0], p->ev[1], p->ev[2], p->ev[3], p->ev_fft0, p->ev_phase0};
+  const cudaEvent_t stop[RICK_NUM_STAGES] = {p->ev[1], p->ev[2], p->ev[3], p->ev[4], p->ev[5], p->ev[6]};
+  for (int k = 0; k < n && k < RICK_NUM_STAGES; k++) {
+    ms[k] = -1.0f;
+    if (p->ran[k]) RICK_CUDA(cudaEventElapsedTime(&ms[k], start[k], stop[k]));
+  }
+  return RICK_OK;
+}
 
 const char *rick_last_error_message(void) { return g_msg; }
 

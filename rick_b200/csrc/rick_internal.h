@@ -99,7 +99,7 @@ void make_table(int kernel, int support, double *tab);
 int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
              const double *vv, const double *ww, const float *weight, const float *vis_re,
              const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
-             uint32_t max_chunk, cudaStream_t st);
+             uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid = nullptr);
 int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
                int accumulate, uint32_t max_chunk, cudaStream_t st);
 void phase_tables(int xaxis, int yaxis, int xaxistot, int yaxistot, double resolution,
