@@ -58,6 +58,10 @@ def parse():
                     help="keep this leading fraction of the time steps (debug only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--forms", default="fp64,mixed",
+                    help="comma list of precision forms to time (fp64 first is the headline)")
+    ap.add_argument("--grid", type=int, default=0, help="override the grid size (profiling cases)")
+    ap.add_argument("--w-planes", type=int, default=0, help="override the w-planes (profiling)")
     return ap.parse_args()
 
 
@@ -169,8 +173,8 @@ def run_ours(args):
     nvis = n * nv
     res = R.resolution_of(obs.meta)
     wmin, wmax = obs.meta["wmin"], obs.meta["wmax"]
-    nx = ny = cfg.grid
-    nw = cfg.w_planes
+    nx = ny = args.grid or cfg.grid
+    nw = args.w_planes or cfg.w_planes
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -190,10 +194,12 @@ def run_ours(args):
         torch.cuda.synchronize()
         launches0 = R.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push(f"{precision}_timed")
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         launches = R.launch_count() - launches0
         ms = e0.elapsed_time(e1) / args.steps
@@ -215,12 +221,16 @@ def run_ours(args):
         image = img.clone()
         return plan, image, ms, stage, stats, launches, lat
 
+    forms = args.forms.split(",")
     with ClockSampler(local) as clocks:
         plan64, img64, ms64, stage64, stats64, launches, lat64 = run_form("fp64")
     plan64.close()
-    planmx, imgmx, msmx, stagemx, statsmx, _, latmx = run_form("mixed")
-    err_mixed = float(torch.linalg.vector_norm(imgmx - img64) / torch.linalg.vector_norm(img64))
-    planmx.close()
+    if "mixed" in forms:
+        planmx, imgmx, msmx, stagemx, statsmx, _, latmx = run_form("mixed")
+        err_mixed = float(torch.linalg.vector_norm(imgmx - img64) / torch.linalg.vector_norm(img64))
+        planmx.close()
+    else:
+        msmx, stagemx, latmx, err_mixed = float("nan"), {}, [float("nan")], None
 
     # max over ranks
     t = torch.tensor([ms64, msmx], dtype=torch.float64, device=dev)
@@ -289,12 +299,13 @@ def run_ours(args):
                            "stages_ms": stage64,
                            "p50_ms": float(np.percentile(lat64, 50)),
                            "p99_ms": float(np.percentile(lat64, 99))},
-                  "mixed": {"vis_per_s": world * nvis / (msmx * 1e-3), "ms": msmx,
-                            "stages_ms": stagemx,
-                            "p50_ms": float(np.percentile(latmx, 50)),
-                            "p99_ms": float(np.percentile(latmx, 99)),
-                            "rel_l2_vs_fp64": err_mixed},
-                  "mixed_over_fp64": ms64 / msmx},
+                  "mixed": None if "mixed" not in forms else {
+                      "vis_per_s": world * nvis / (msmx * 1e-3), "ms": msmx,
+                      "stages_ms": stagemx,
+                      "p50_ms": float(np.percentile(latmx, 50)),
+                      "p99_ms": float(np.percentile(latmx, 99)),
+                      "rel_l2_vs_fp64": err_mixed},
+                  "mixed_over_fp64": (ms64 / msmx) if "mixed" in forms else None},
         "job": {"rows_gridded": stats64["rows_gridded"], "rows_dropped": stats64["rows_dropped"],
                 "records": stats64["records"], "work_items": stats64["work_items"],
                 "generate_s": gen_s},
