@@ -176,6 +176,29 @@ int rick_plan_get_stats(rick_plan *plan, rick_plan_stats *stats); /* synchronise
 int rick_plan_set_timing(rick_plan *plan, int on);
 int rick_plan_stage_ms(rick_plan *plan, float *ms, int n);
 
+/* ---- 3. gridding without device allocation ------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory at run time -- real-time pipelines that reserve all GPU memory at
+ * start-up and may not grow it inside their streaming loop, or host frameworks
+ * that own the device memory pool -- this grids device-resident rows
+ * (wstack's arguments, as device pointers, all rows gridded) into the caller's
+ * device cube grid[2*Nw*Ny*Nx] (overwritten) without calling cudaMalloc: its
+ * scratch is one static __device__ array of 32 MiB that every GPU loading the
+ * library holds until exit.  A job whose scratch does not fit is rejected with
+ * RICK_ERR_INVALID_ARG (rick_wstack_noalloc_capacity gives the row limit for a
+ * geometry).  All calls share that array and it keeps the last call's
+ * contents; calls whose GPU work overlaps race on it.  The first call on a
+ * device looks up the array's device address, so make it before any stream
+ * capture.  Asynchronous on `stream`. */
+int rick_wstack_noalloc(int num_w_planes, uint64_t num_points, uint32_t freq_per_chan,
+                        uint32_t polarizations, const double *uu, const double *vv,
+                        const double *ww, const float *vis_real, const float *vis_img,
+                        const float *weight, double dx, double dw, int w_support, int kernel,
+                        int grid_size_x, int grid_size_y, double *grid, void *stream);
+int rick_wstack_noalloc_capacity(int num_w_planes, int grid_size_x, int grid_size_y,
+                                 uint64_t *max_rows);
+
 /* Names of the kernels this library launches, and how many launches it has
  * issued in this process (for launch accounting). */
 int rick_kernel_names(const char **names, int max_names);
