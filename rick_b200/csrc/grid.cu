@@ -13,6 +13,8 @@
 //   as norm*exp(-u^2*std22)*exp(-v^2*std22)).
 // Table indices are computed with round-to-nearest intrinsics in FP64 from the
 // exact fractional position, so they equal the reference's indices bit for bit.
+#include <algorithm>
+
 #include "rick_internal.h"
 
 namespace rick {
@@ -33,11 +35,11 @@ __global__ void __launch_bounds__(kGridThreads)
                  const uint32_t *__restrict__ item_off, uint32_t nbins, uint32_t max_chunk,
                  Geometry g, int kernel, const double *__restrict__ table, int accumulate,
                  uint64_t *__restrict__ counters,
-                 typename Vec2<OutT>::type *__restrict__ cube) {
+                 typename Vec2<OutT>::type *__restrict__ cube, uint32_t *__restrict__ rowmask) {
   __shared__ double s_re[kTile * kPitch];
   __shared__ double s_im[kTile * kPitch];
   __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
-  __shared__ uint32_t s_item, s_bin, s_first, s_nitems;
+  __shared__ uint32_t s_item, s_bin, s_first, s_nitems, s_rows;
 
   const int ntab = kIncreasePrecision * g.support;
   for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = table[t];
@@ -67,6 +69,7 @@ __global__ void __launch_bounds__(kGridThreads)
       }
       s_item = item;
       s_bin = bin;
+      s_rows = 0;
     }
     for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
       s_re[c] = 0.0;
@@ -111,6 +114,16 @@ __global__ void __launch_bounds__(kGridThreads)
       }
       const int j = q.gu - g.half + (int)d;
       const bool col_ok = valid && (int)d < g.support && j >= 0 && j < g.nx && j >= x0 && j < x0 + kTile;
+      if (rowmask && valid && d == 0) {
+        // grid rows of this tile the record's footprint reaches
+        const int lo = max(max(q.gv - g.half, 0), y0);
+        const int hi = min(min(q.gv + g.half, g.ny - 1), y0 + kTile - 1);
+        if (lo <= hi) {
+          const uint32_t span = (uint32_t)(hi - lo + 1);
+          const uint32_t bits = (span >= 32u ? 0xffffffffu : ((1u << span) - 1u)) << (lo - y0);
+          atomicOr(&s_rows, bits);
+        }
+      }
       const double su = hi ? gnorm * wu : wu;
       for (int e = 0; e < g.support; e++) {
         const double wve = __shfl_sync(kFull, wv, grp_base + e);
@@ -125,7 +138,8 @@ __global__ void __launch_bounds__(kGridThreads)
     }
     __syncthreads();
 
-    // Flush the tile.
+    // Flush the tile (and the rows it touched).
+    if (rowmask && threadIdx.x == 0 && s_rows) atomicOr(&rowmask[(uint64_t)w * g.nty + ty], s_rows);
     const uint64_t plane = (uint64_t)g.nx * g.ny;
     for (int c = threadIdx.x; c < kTile * kTile; c += blockDim.x) {
       const int y = c / kTile, x = c % kTile;
@@ -154,9 +168,35 @@ __global__ void __launch_bounds__(kGridThreads)
   }
 }
 
+// Tiles split over several work items receive their parts with atomics, so
+// they must start at zero when the cube is not cleared as a whole.
+template <typename OutT>
+__global__ void k_zero_split_tiles(const uint32_t *__restrict__ item_off, uint32_t nbins, Geometry g,
+                                   typename Vec2<OutT>::type *__restrict__ cube) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  const uint64_t plane = (uint64_t)g.nx * g.ny;
+  for (uint64_t b = warp; b < nbins; b += nwarps) {
+    if (item_off[b + 1] - item_off[b] <= 1) continue;
+    const int tx = (int)(b % (uint32_t)g.ntx);
+    const int ty = (int)((b / (uint32_t)g.ntx) % (uint32_t)g.nty);
+    const int w = (int)(b / ((uint64_t)g.ntx * g.nty));
+    const int gx = tx * kTile + (int)lane;
+    if (gx >= g.nx) continue;
+    typename Vec2<OutT>::type z;
+    z.x = 0;
+    z.y = 0;
+    for (int y = 0; y < kTile; y++) {
+      const int gy = ty * kTile + y;
+      if (gy < g.ny) cube[(uint64_t)w * plane + (uint64_t)gy * g.nx + gx] = z;
+    }
+  }
+}
+
 template <typename OutT>
 int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accumulate,
-                uint32_t max_chunk, cudaStream_t st) {
+                uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask) {
   const int sms = num_sms();
   using V = typename Vec2<OutT>::type;
   const uint32_t nbins = (uint32_t)g.nbins();
@@ -166,11 +206,13 @@ int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accum
   if (g.support <= 8)
     k_grid_tiles<OutT, 8><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
                                                            nbins, max_chunk, g, kernel, s.table,
-                                                           accumulate, s.counters, (V *)cube);
+                                                           accumulate, s.counters, (V *)cube,
+                                                           rowmask);
   else
     k_grid_tiles<OutT, 16><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
                                                             nbins, max_chunk, g, kernel, s.table,
-                                                            accumulate, s.counters, (V *)cube);
+                                                            accumulate, s.counters, (V *)cube,
+                                                            rowmask);
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
@@ -178,9 +220,25 @@ int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accum
 }  // namespace
 
 int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
-               int accumulate, uint32_t max_chunk, cudaStream_t st) {
-  if (precision == RICK_PREC_FP64) return launch_grid<double>(g, kernel, s, cube, accumulate, max_chunk, st);
-  return launch_grid<float>(g, kernel, s, cube, accumulate, max_chunk, st);
+               int accumulate, uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask) {
+  if (precision == RICK_PREC_FP64)
+    return launch_grid<double>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask);
+  return launch_grid<float>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask);
+}
+
+int zero_split_tiles(const Geometry &g, int precision, Scratch &s, void *cube, cudaStream_t st) {
+  const uint32_t nbins = (uint32_t)g.nbins();
+  const int blocks = (int)std::min<uint64_t>(((uint64_t)nbins * 32 + 255) / 256,
+                                             (uint64_t)num_sms() * 16);
+  RICK_LAUNCHED();
+  if (precision == RICK_PREC_FP64)
+    k_zero_split_tiles<double><<<std::max(blocks, 1), 256, 0, st>>>(s.item_off, nbins, g,
+                                                                    (double2 *)cube);
+  else
+    k_zero_split_tiles<float><<<std::max(blocks, 1), 256, 0, st>>>(s.item_off, nbins, g,
+                                                                   (float2 *)cube);
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
 }
 
 }  // namespace rick

@@ -4,6 +4,7 @@
 // except rick_plan_image_host and rick_plan_get_stats.
 #include <math.h>
 #include <stdarg.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -111,7 +112,9 @@ __global__ void k_import_cube(const double *__restrict__ src, float *__restrict_
 
 using namespace rick;
 
-enum CubeState { kCubeRaw = 0, kCubeTransformed = 1, kCubeNormalised = 2 };
+// kCubeSparse: after the fused imaging call the cube holds row-transformed
+// touched rows only; it is not a valid input to export, FFT or phase.
+enum CubeState { kCubeRaw = 0, kCubeTransformed = 1, kCubeNormalised = 2, kCubeSparse = 3 };
 
 struct rick_plan {
   rick_plan_desc d{};
@@ -143,6 +146,9 @@ struct rick_plan {
   cudaEvent_t ev[RICK_NUM_STAGES + 1] = {};
   bool ran[RICK_NUM_STAGES] = {};
   cudaEvent_t ev_fft0 = nullptr, ev_phase0 = nullptr;
+  // sparse-aware FFT (power-of-two axes)
+  bool sparse = false;
+  FftScratch f{};
 };
 
 namespace {
@@ -272,7 +278,8 @@ int mark(rick_plan *p, cudaEvent_t e, cudaStream_t st) {
 
 int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
                    const double *ww, const float *weight, const float *vis_re, const float *vis_im,
-                   int select, int accumulate, double dx, double dw, cudaStream_t st) {
+                   int select, int accumulate, double dx, double dw, cudaStream_t st,
+                   bool sparse = false) {
   if (nrows > p->d.max_rows)
     return set_error(RICK_ERR_INVALID_ARG, "nrows %llu exceeds the plan capacity %llu",
                      (unsigned long long)nrows, (unsigned long long)p->d.max_rows);
@@ -287,20 +294,51 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
                     p->d.freq_per_chan, p->d.polarizations, p->s, chunk, st,
                     p->timing ? p->ev[1] : nullptr));
   RICK_TRY(mark(p, p->ev[2], st));
-  if (!accumulate) RICK_CUDA(cudaMemsetAsync(p->cube, 0, p->cube_vals * p->val_bytes, st));
+  if (sparse) {
+    // only the tiles several work items add into are cleared; the row mask
+    // records which grid rows the footprints reach
+    RICK_CUDA(cudaMemsetAsync(p->f.rowmask, 0, (size_t)p->g.nw * p->g.nty * 4, st));
+    RICK_TRY(zero_split_tiles(p->g, p->d.precision, p->s, p->cube, st));
+  } else if (!accumulate) {
+    RICK_CUDA(cudaMemsetAsync(p->cube, 0, p->cube_vals * p->val_bytes, st));
+  }
   RICK_TRY(mark(p, p->ev[3], st));
-  RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, chunk, st));
+  RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, chunk, st,
+                      sparse ? p->f.rowmask : nullptr));
   RICK_TRY(mark(p, p->ev[4], st));
   p->ran[0] = p->ran[1] = p->ran[3] = true;
   p->ran[2] = !accumulate;
-  p->cube_state = kCubeRaw;
+  p->cube_state = sparse ? kCubeSparse : kCubeRaw;
   p->last_rows = nrows;
+  return RICK_OK;
+}
+
+// grid -> touched-row FFT -> column FFT fused with the w-correction.
+int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+                      const double *ww, const float *weight, const float *vis_re,
+                      const float *vis_im, int select, double resolution, double wmin,
+                      double wmax, double *img_re, double *img_im, cudaStream_t st) {
+  RICK_TRY(plan_grid_impl(p, nrows, uu, vv, ww, weight, vis_re, vis_im, select, 0,
+                          1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, st, true));
+  RICK_TRY(mark(p, p->ev_fft0, st));
+  RICK_TRY(sparse_row_list(p->f, p->g, st));
+  RICK_TRY(sparse_fft_rows(p->d.precision, p->f, p->cube, p->g, p->s.bin_count, st));
+  RICK_TRY(mark(p, p->ev[5], st));
+  const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
+  RICK_TRY(ensure_lm(p, nx, ny, nx, ny, resolution, st));
+  RICK_TRY(mark(p, p->ev_phase0, st));
+  const double norm = 1.0 / (double)((long long)nx * ny);  // fourier_transform.c:24
+  RICK_TRY(sparse_fft_cols_image(p->d.precision, p->f, p->cube, p->g, p->d_lm, p->d_lm + nx, wmin,
+                                 wmax, norm, p->d.phase_on, img_re, img_im, st));
+  RICK_TRY(mark(p, p->ev[6], st));
+  p->ran[4] = p->ran[5] = true;
+  p->cube_state = kCubeSparse;
   return RICK_OK;
 }
 
 int plan_fft_impl(rick_plan *p, cudaStream_t st) {
   if (p->cube_state != kCubeRaw)
-    return set_error(RICK_ERR_INVALID_ARG, "cube already transformed");
+    return set_error(RICK_ERR_INVALID_ARG, "the cube is not a gridded (untransformed) cube");
   if (!p->fft) RICK_TRY(choose_fft(p));
   RICK_CUFFT(cufftSetStream(p->fft, st));
   RICK_TRY(mark(p, p->ev_fft0, st));
@@ -330,7 +368,7 @@ double cube_scale(const rick_plan *p) {
 int plan_phase_impl(rick_plan *p, int xtot, int ytot, double resolution, double wmin,
                     double wmax, double *img_re, double *img_im, int accumulate,
                     cudaStream_t st) {
-  if (p->cube_state == kCubeRaw)
+  if (p->cube_state == kCubeRaw || p->cube_state == kCubeSparse)
     return set_error(RICK_ERR_INVALID_ARG, "phase correction needs a transformed cube");
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
   RICK_TRY(ensure_lm(p, nx, ny, xtot, ytot, resolution, st));
@@ -353,6 +391,7 @@ int rick_plan_footprint(const rick_plan_desc *desc, uint64_t *bytes) {
   const uint64_t nbins = nw * ((nx + kTile - 1) / kTile) * ((ny + kTile - 1) / kTile);
   const uint64_t vb = desc->precision == RICK_PREC_FP64 ? 8 : 4;
   uint64_t b = 2 * nw * nx * ny * vb;                      // cube
+  if (sparse_fft_supported((int)nx, (int)ny)) b *= 2;      // + column-blocked planes
   b += std::max<uint64_t>(b / 4, 512ull << 20);            // FFT work (upper bound)
   b += 4 * (nbins + 1) * 4 + 4 * scan_tmp_words(nbins + 1);  // bins, items, cursor, scan
   b += 4 * desc->max_rows * sizeof(RecF64);                // records
@@ -404,6 +443,37 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
                                cudaMemcpyHostToDevice);
     if (e != cudaSuccess) st = cuda_status(e, "cudaMemcpy(table)", __FILE__, __LINE__);
   }
+  p->sparse = sparse_fft_supported(desc->grid_size_x, desc->grid_size_y) &&
+              getenv("RICK_DENSE_FFT") == nullptr;
+  if (st == RICK_OK && p->sparse) {
+    const int nx = desc->grid_size_x, ny = desc->grid_size_y;
+    A((void **)&p->f.rowmask, (size_t)desc->num_w_planes * p->g.nty * 4);
+    A((void **)&p->f.rowlist, (size_t)desc->num_w_planes * ny * 4);
+    A((void **)&p->f.counts, (size_t)(1 + desc->num_w_planes) * 4);
+    A((void **)&p->f.tw_x64, (size_t)nx * sizeof(double2));
+    A((void **)&p->f.tw_y64, (size_t)ny * sizeof(double2));
+    A((void **)&p->f.tw_x32, (size_t)nx * sizeof(float2));
+    A((void **)&p->f.tw_y32, (size_t)ny * sizeof(float2));
+    A(&p->f.blocked, p->cube_vals * p->val_bytes);
+    if (st == RICK_OK) {
+      const int nmax = std::max(nx, ny);
+      double2 *t64 = (double2 *)malloc(sizeof(double2) * nmax);
+      float2 *t32 = (float2 *)malloc(sizeof(float2) * nmax);
+      if (!t64 || !t32) st = set_error(RICK_ERR_NOT_ENOUGH_MEM, "host twiddle tables");
+      for (int axis = 0; axis < 2 && st == RICK_OK; axis++) {
+        const int n = axis == 0 ? nx : ny;
+        make_twiddles(n, t64, t32);
+        cudaError_t e = cudaMemcpy(axis == 0 ? p->f.tw_x64 : p->f.tw_y64, t64, sizeof(double2) * n,
+                                   cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+          e = cudaMemcpy(axis == 0 ? p->f.tw_x32 : p->f.tw_y32, t32, sizeof(float2) * n,
+                         cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaMemcpy(twiddles)", __FILE__, __LINE__);
+      }
+      free(t64);
+      free(t32);
+    }
+  }
   if (st == RICK_OK) st = choose_fft(p);
   if (st != RICK_OK) {
     rick_plan_destroy(p);
@@ -420,7 +490,8 @@ int rick_plan_destroy(rick_plan *p) {
   if (p->fft) cufftDestroy(p->fft);
   void *ptrs[] = {p->cube, p->s.bin_count, p->s.bin_cursor, p->s.item_off, p->s.scan_tmp,
                   p->s.counters, p->s.records, p->s.table, p->d_lm, p->fft_work, p->h_rows_d,
-                  p->d_img, p->d_stage};
+                  p->d_img, p->d_stage, p->f.rowmask, p->f.rowlist, p->f.counts,
+                  p->f.tw_x64, p->f.tw_y64, p->f.tw_x32, p->f.tw_y32, p->f.blocked};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->h_lm) cudaFreeHost(p->h_lm);
@@ -463,6 +534,10 @@ int rick_plan_image(rick_plan *p, uint64_t nrows, const double *uu, const double
   if (!p || !image_real || !image_imag) return set_error(RICK_ERR_INVALID_ARG, "null argument");
   DeviceGuard guard(p->device);
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->sparse)
+    return plan_image_sparse(p, nrows, uu, vv, ww, weight, vis_real, vis_img,
+                             row_selection == RICK_ROWS_SECTOR0, resolution, wmin, wmax,
+                             image_real, image_imag, st);
   RICK_TRY(plan_grid_impl(p, nrows, uu, vv, ww, weight, vis_real, vis_img,
                           row_selection == RICK_ROWS_SECTOR0, 0, 1.0 / p->d.grid_size_x,
                           1.0 / p->d.num_w_planes, st));
@@ -534,6 +609,9 @@ int rick_plan_image_host(rick_plan *p, uint64_t nrows, const double *uu, const d
 
 int rick_plan_export_cube(rick_plan *p, double *dst, int dst_is_host, void *stream) {
   if (!p || !dst) return set_error(RICK_ERR_INVALID_ARG, "null argument");
+  if (p->cube_state == kCubeSparse)
+    return set_error(RICK_ERR_INVALID_ARG,
+                     "rick_plan_image keeps no full cube; grid with rick_plan_grid to export it");
   DeviceGuard guard(p->device);
   cudaStream_t st = (cudaStream_t)stream;
   const double scale = cube_scale(p);
