@@ -31,6 +31,12 @@ template <typename T> struct V2;
 template <> struct V2<double> { using t = double2; };
 template <> struct V2<float> { using t = float2; };
 
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
 template <typename T> struct Cx {
   T re, im;
 };
@@ -126,14 +132,18 @@ __device__ __forceinline__ void cp_async_wait() {
 
 constexpr int kVpt = 8;  // values per thread
 
-// Column-blocked layout of the row-transformed planes: 128-byte blocks of
-// columns, each block holding every row: element (w, k, n) sits at
+// Row-transformed planes are stored column-blocked: 128-byte blocks of
+// columns, each block holding every row -- element (w, k, n) sits at
 //   ((w * (nx / CB) + n / CB) * ny + k) * CB + n % CB,   CB = 128 / sizeof(complex).
-// Row-pass writes are whole 128-byte lines; the column pass of the CB columns
-// of a block streams one contiguous region per plane.
-template <typename T> __host__ __device__ constexpr int col_block() { return 128 / (int)sizeof(typename V2<T>::t); }
+// Row-pass writes are whole 128-byte lines; the CB CTAs that transform the
+// columns of one block stream one contiguous region per plane and share its
+// lines in L2.
+template <typename T> __host__ __device__ constexpr int col_block() {
+  return 128 / (int)sizeof(typename V2<T>::t);
+}
 template <typename T>
-__device__ __forceinline__ uint64_t blocked_index(uint32_t w, uint32_t k, uint32_t n, int nx, int ny) {
+__device__ __forceinline__ uint64_t blocked_index(uint32_t w, uint32_t k, uint32_t n, int nx,
+                                                  int ny) {
   constexpr int CB = col_block<T>();
   return (((uint64_t)w * (nx / CB) + n / CB) * ny + k) * CB + (n % CB);
 }
@@ -188,6 +198,70 @@ __device__ __forceinline__ void stockham_pass(typename V2<T>::t *s, int t, int N
   __syncthreads();
 }
 
+// The last Stockham pass (Ns * R == N) with its outputs kept in registers:
+// thread t's butterflies write positions t + q*G, q = b + B*r, so out[q] is the
+// transform's value at index t + q*G -- exactly the points the thread owns next.
+template <typename T, int N, int R>
+__device__ __forceinline__ void stockham_last_pass(const typename V2<T>::t *s, int t,
+                                                   const typename V2<T>::t *__restrict__ tw,
+                                                   Cx<T> out[kVpt]) {
+  constexpr int G = N / kVpt, B = kVpt / R, Ns = N / R;
+  Cx<T> v[B][R];
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * G;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[b][r] = lds<T>(s, j + r * (N / R));
+  }
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * G;  // j < Ns, so jm = j and the output index is j + r*Ns
+    if (Ns > 1) {
+      const typename V2<T>::t *twp = tw + (Ns - 1) + j;
+      if (R == 8) {
+        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
+        const Cx<T> w1 = {a.x, a.y}, w2 = {b2.x, b2.y}, w4 = {b4.x, b4.y};
+        const Cx<T> w3 = cmul<T>(w1, w2.re, w2.im);
+        const Cx<T> w5 = cmul<T>(w1, w4.re, w4.im);
+        const Cx<T> w6 = cmul<T>(w2, w4.re, w4.im);
+        const Cx<T> w7 = cmul<T>(w3, w4.re, w4.im);
+        const Cx<T> w[8] = {{(T)1, (T)0}, w1, w2, w3, w4, w5, w6, w7};
+#pragma unroll
+        for (int r = 1; r < R; r++) v[b][r] = cmul<T>(v[b][r], w[r].re, w[r].im);
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+          const typename V2<T>::t w = __ldg(twp + (r - 1) * Ns);
+          v[b][r] = cmul<T>(v[b][r], w.x, w.y);
+        }
+      }
+    }
+    Dft<T, R>::run(v[b]);
+#pragma unroll
+    for (int r = 0; r < R; r++) out[b + B * r] = v[b][r];
+  }
+}
+
+// Inverse FFT of N = 2^LOGN points held in shared memory; the result of the
+// last pass stays in registers (out[q] = value at t + q*G).  The buffer may be
+// overwritten after the caller's next barrier.
+template <typename T, int LOGN>
+__device__ __forceinline__ void fft_to_regs(typename V2<T>::t *s, int t,
+                                            const typename V2<T>::t *__restrict__ tw,
+                                            Cx<T> out[kVpt]) {
+  constexpr int N = 1 << LOGN;
+  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+  constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
+  constexpr int NPASS = P8 + (REM ? 1 : 0);
+  int Ns = 1;
+#pragma unroll
+  for (int p = 0; p < NPASS - 1; p++) {
+    stockham_pass<T, N, 8>(s, t, Ns, tw);
+    Ns *= 8;
+  }
+  stockham_last_pass<T, N, LASTR>(s, t, tw, out);
+}
+
 // Whole inverse FFT of N = 2^LOGN points (unnormalised), in place.
 template <typename T, int LOGN>
 __device__ __forceinline__ void fft_inplace(typename V2<T>::t *s, int t,
@@ -209,21 +283,24 @@ template <int LOGN> constexpr int block_threads() {
   return group_threads<LOGN>() > 256 ? group_threads<LOGN>() : 256;
 }
 
-// Row pass: inverse FFT along x of the listed (plane, row) pairs, from the
-// gridded cube (tiles without records read as zeros) into the column-blocked
-// buffer.
+// Row pass: inverse FFT along x of the listed touched rows, from the gridded
+// cube into the column-blocked buffer.  Tiles that received no record (bit
+// clear in the band's tile bitmap) were never written and read as zeros.  The
+// last FFT pass leaves each thread's outputs in registers, stored as whole
+// 128-byte lines.
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(block_threads<LOGN>())
     k_fft_rows(const typename V2<T>::t *__restrict__ cube, typename V2<T>::t *__restrict__ out,
-               int nx, int ny, int nty, int ntx, const uint32_t *__restrict__ rowlist,
-               const uint32_t *__restrict__ counts, const uint32_t *__restrict__ bin_off,
+               int nx, int ny, int nty, int tmw, const uint32_t *__restrict__ tilemask,
+               const uint32_t *__restrict__ rowlist, const uint32_t *__restrict__ counts,
                const typename V2<T>::t *__restrict__ tw) {
-  constexpr int N = 1 << LOGN, G = N / kVpt;
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  using V = typename V2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  typename V2<T>::t *s = reinterpret_cast<typename V2<T>::t *>(smem_raw);
-  const int rpc = blockDim.x / G;
+  V *s = reinterpret_cast<V *>(smem_raw);
+  const int rpc = blockDim.x / G;  // rows per CTA
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
-  typename V2<T>::t *srow = s + grp * (N + N / 16);
+  V *srow = s + grp * LEN;
   const uint32_t nrows = counts[0];
   for (uint32_t base = blockIdx.x * rpc; base < nrows; base += gridDim.x * rpc) {
     const uint32_t li = base + grp;
@@ -234,27 +311,27 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
       w = rid / (uint32_t)ny;
       k = rid % (uint32_t)ny;
     }
+    const uint32_t *tm = tilemask + ((uint64_t)w * nty + (k >> 5)) * tmw;
     const uint64_t rowbase = ((uint64_t)w * ny + k) * nx;
-    const uint32_t binbase = (w * (uint32_t)nty + (k >> 5)) * (uint32_t)ntx;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int x = t + q * G;
-      typename V2<T>::t v;
+      V v;
       v.x = 0;
       v.y = 0;
-      if (active) {
-        const uint32_t b = binbase + (x >> 5);
-        if (bin_off[b + 1] != bin_off[b]) v = cube[rowbase + x];  // tile holds records
-      }
+      if (active && ((tm[x >> 10] >> ((x >> 5) & 31)) & 1u)) v = cube[rowbase + x];
       srow[pad(x)] = v;
     }
     __syncthreads();
-    fft_inplace<T, LOGN>(srow, t, tw);
+    Cx<T> res[kVpt];
+    fft_to_regs<T, LOGN>(srow, t, tw, res);
     if (active) {
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
-        const int x = t + q * G;
-        out[blocked_index<T>(w, k, x, nx, ny)] = srow[pad(x)];
+        V v;
+        v.x = res[q].re;
+        v.y = res[q].im;
+        out[blocked_index<T>(w, k, t + q * G, nx, ny)] = v;
       }
     }
     __syncthreads();
@@ -264,12 +341,17 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
 // Column pass fused with the w-correction and the plane sum: each row group
 // owns one image column and walks the planes in increasing w.  With DB the
 // next plane's column is copied into a second shared buffer (cp.async,
-// untouched rows zero-filled) while the current one is transformed.
-// sqrt(1 - l^2 - m^2) of the column's pixels is formed once per column
-// (shared memory).  The plain form evaluates every plane's phase with sincos
-// of the reference's argument; with RECUR (mixed form) the phase advances from
-// plane to plane by a per-pixel step exp(i 2 pi dw (root - 1)) kept in shared
-// memory, re-anchored with an exact sincos every kAnchor planes.
+// untouched rows zero-filled) while the current one is transformed; the last
+// FFT pass leaves the column's values in the registers of the threads that
+// accumulate those pixels.
+//
+// Phase (phase_correction.cu:51-80): every kAnchor planes (and at the first
+// plane; at every plane without RECUR, when the step table does not fit) the factor exp(i*(2 pi wterm)*(root-1)) is evaluated with sincos of the
+// reference's FP64 argument and scaled by dwnorm*root; between anchors it
+// advances by the per-pixel step exp(i*(2 pi dw)*(root-1)) (shared memory).
+// Over 8 planes the advanced factor differs from a long-double evaluation by
+// < 1e-13 per pixel at the w range of a 4096^2 x 32-plane LOFAR-like image --
+// less than the rounding of the reference's own argument (~3e-13).
 constexpr int kAnchor = 8;
 
 template <typename T, int LOGN, bool DB, bool RECUR>
@@ -287,19 +369,25 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
   const int rpc = blockDim.x / G;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
   V *buf[2] = {s + grp * LEN, s + (DB ? rpc + grp : grp) * LEN};
-  double *sroot = reinterpret_cast<double *>(s + (DB ? 2 : 1) * rpc * LEN) + grp * N;
-  double2 *sstep = reinterpret_cast<double2 *>(reinterpret_cast<double *>(s + (DB ? 2 : 1) * rpc * LEN) + rpc * N) + grp * N;
+  double2 *tables = reinterpret_cast<double2 *>(s + (DB ? 2 : 1) * rpc * LEN);
+  double2 *sstep = tables + grp * N;  // RECUR only
+  // row masks of the next two planes to load (the CTA's columns share them)
+  uint32_t *smask = reinterpret_cast<uint32_t *>(tables + (RECUR ? rpc * N : 0));
   const bool phase = phase_on && nw > 1;
   const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
   auto next_plane = [&](int iw) {
     do { iw++; } while (iw < nw && counts[1 + iw] == 0);  // planes without data add exact zeros
     return iw;
   };
-  auto load_column = [&](V *dst, int iw, uint32_t n, bool active) {
-    const uint32_t *mask = rowmask + (uint64_t)iw * nty;
+  auto stage_mask = [&](int slot, int iw) {
+    if (iw < nw)
+      for (int i = threadIdx.x; i < nty; i += blockDim.x)
+        smask[slot * nty + i] = rowmask[(uint64_t)iw * nty + i];
+  };
+  auto load_column = [&](V *dst, int iw, int slot, uint32_t n, bool active) {
+    const uint32_t *mask = smask + slot * nty;
     constexpr int CB = col_block<T>();
-    const uint32_t nn = active ? n : 0;
-    const V *col = cube + blocked_index<T>(iw, 0, nn, nx, ny);  // row k at col + k * CB
+    const V *col = cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);  // row k at k * CB
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int k = t + q * G;
@@ -315,68 +403,74 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
       }
     }
   };
+  // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits
+  auto root_of = [&](double l, int m) {
+    const double mm = mtab[m];
+    return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
+  };
   const double dwstep = __dmul_rn(twopi, dw);
   for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)nx; base += gridDim.x * rpc) {
     const uint32_t n = base + grp;
     const bool active = n < (uint32_t)nx;
+    const double l = active ? ltab[n] : 0.0;
     double acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
 #pragma unroll
     for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = 0.0;
     int iw = next_plane(-1);
-    int cur = 0;
-    if (DB && iw < nw) {
-      load_column(buf[0], iw, n, active);
-      cp_async_commit();
-    }
-    if (phase) {
-      // phase_correction.cu:56-64 per pixel of this column, once
-      const double l = active ? ltab[n] : 0.0;
+    int nxt = next_plane(iw);
+    stage_mask(0, iw);
+    stage_mask(1, nxt);
+    if (phase && RECUR) {
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int m = t + q * G;
-        const double mm = mtab[m];
-        const double radius2 = __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm));
-        const double root = __dsqrt_rn(__dsub_rn(1.0, radius2));
-        sroot[m] = root;
-        if (RECUR) {
-          double sn, cs;
-          sincos(__dmul_rn(dwstep, __dsub_rn(root, 1.0)), &sn, &cs);
-          sstep[m] = make_double2(cs, sn);
-        }
+        double sn, cs;
+        sincos(__dmul_rn(dwstep, __dsub_rn(root_of(l, m), 1.0)), &sn, &cs);
+        sstep[m] = make_double2(cs, sn);
       }
     }
+    __syncthreads();
+    if (DB && iw < nw) {
+      load_column(buf[0], iw, 0, n, active);
+      cp_async_commit();
+    }
+    int cur = 0, it = 0;
     int last_anchor = -kAnchor, prev_iw = -1;
     while (iw < nw) {
-      const int nxt = next_plane(iw);
+      const int nn = next_plane(nxt);  // plane after the next one
       if (DB) {
-        if (nxt < nw) load_column(buf[cur ^ 1], nxt, n, active);
+        if (nxt < nw) load_column(buf[cur ^ 1], nxt, (it + 1) & 1, n, active);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
-        load_column(buf[0], iw, n, active);
+        load_column(buf[0], iw, it & 1, n, active);
       }
       __syncthreads();
-      V *scol = buf[cur];
-      fft_inplace<T, LOGN>(scol, t, tw);
-      // phase_correction.cu:51-80 for pixel (m, n) of plane iw
-      const double wterm = __dadd_rn(wmin, __dmul_rn((double)iw, dw));
-      const double cw = __dmul_rn(twopi, wterm);
+      // this plane's mask slot is free now: stage the plane after next
+      stage_mask(it & 1, nn);
+      Cx<T> x[kVpt];
+      fft_to_regs<T, LOGN>(buf[cur], t, tw, x);
       const bool anchor = !RECUR || iw - last_anchor >= kAnchor;
-      const int gap = iw - prev_iw;  // planes since the previous phase (empty planes are skipped)
-      if (anchor) last_anchor = iw;
+      const int gap = iw - prev_iw;  // planes since the previous factor (empty planes skipped)
+      double cw = 0.0;
+      if (anchor) {
+        last_anchor = iw;
+        cw = __dmul_rn(twopi, __dadd_rn(wmin, __dmul_rn((double)iw, dw)));  // 2 pi wterm
+      }
       prev_iw = iw;
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int m = t + q * G;
-        const Cx<T> x = lds<T>(scol, m);
-        const double p = __dmul_rn(norm, (double)x.re), qq = __dmul_rn(norm, (double)x.im);
+        const double p = __dmul_rn(norm, (double)x[q].re), qq = __dmul_rn(norm, (double)x[q].im);
         if (phase) {
-          const double root = sroot[m];
-          double sn, cs;
           if (anchor) {
+            const double root = root_of(l, m);
+            double sn, cs;
             sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+            const double amp = dwnorm * root;
+            ph_re[q] = cs * amp;
+            ph_im[q] = sn * amp;
           } else {
-            // advance by `gap` planes: exp(i gap B), gap >= 1 (empty planes skipped)
             const double2 st = sstep[m];
             double sr = st.x, si = st.y;
             for (int g2 = 1; g2 < gap; g2++) {
@@ -384,15 +478,12 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
               si = sr * st.y + si * st.x;
               sr = tr;
             }
-            cs = ph_re[q] * sr - ph_im[q] * si;
-            sn = ph_re[q] * si + ph_im[q] * sr;
+            const double tr = ph_re[q] * sr - ph_im[q] * si;
+            ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
+            ph_re[q] = tr;
           }
-          if (RECUR) {
-            ph_re[q] = cs;
-            ph_im[q] = sn;
-          }
-          acc_re[q] += (p * cs - qq * sn) * dwnorm * root;
-          acc_im[q] += (p * sn + qq * cs) * dwnorm * root;
+          acc_re[q] += p * ph_re[q] - qq * ph_im[q];
+          acc_im[q] += p * ph_im[q] + qq * ph_re[q];
         } else {
           acc_re[q] += p;
           acc_im[q] += qq;
@@ -401,6 +492,8 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
       __syncthreads();
       if (DB) cur ^= 1;
       iw = nxt;
+      nxt = nn;
+      it++;
     }
     if (DB) cp_async_wait<0>();
     if (active) {
@@ -411,12 +504,12 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
         img_im[(uint64_t)m * nx + n] = acc_im[q];
       }
     }
-    __syncthreads();  // sroot / sstep are rewritten for the next column
+    __syncthreads();  // sstep / smask are rewritten for the next column
   }
 }
 
-// Compacts the row mask into a list of (plane, row) ids and per-plane counts.
-// counts[0] = total rows, counts[1 + w] = rows of plane w.
+// Compacts the row mask into the list of touched (plane, row) ids and per-plane
+// counts: counts[0] = rows, counts[1 + w] = touched rows of plane w.
 __global__ void k_row_list(const uint32_t *__restrict__ rowmask, int nw, int ny, int nty,
                            uint32_t *__restrict__ rowlist, uint32_t *__restrict__ counts) {
   const uint64_t nwords = (uint64_t)nw * nty;
@@ -445,11 +538,9 @@ size_t fft_smem(int rpc) {
 }
 
 template <typename T, int LOGN>
-int launch_rows(FftScratch &f, void *cube, const Geometry &g, const uint32_t *bin_off,
-                cudaStream_t st) {
+int launch_rows(FftScratch &f, void *cube, const Geometry &g, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
-  const int rpc = BT / G;
-  const size_t sm = fft_smem<T, LOGN>(rpc);
+  const size_t sm = fft_smem<T, LOGN>(BT / G);
   RICK_CUDA(cudaFuncSetAttribute(k_fft_rows<T, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sm));
   int per_sm = 0;
@@ -457,8 +548,8 @@ int launch_rows(FftScratch &f, void *cube, const Geometry &g, const uint32_t *bi
   const int blocks = num_sms() * std::max(per_sm, 1);
   RICK_LAUNCHED();
   k_fft_rows<T, LOGN><<<blocks, BT, sm, st>>>(
-      (const typename V2<T>::t *)cube, (typename V2<T>::t *)f.blocked, g.nx, g.ny, g.nty, g.ntx,
-      f.rowlist, f.counts, bin_off,
+      (const typename V2<T>::t *)cube, (typename V2<T>::t *)f.blocked, g.nx, g.ny, g.nty,
+      (g.ntx + 31) / 32, f.tilemask, f.rowlist, f.counts,
       (const typename V2<T>::t *)(sizeof(T) == 8 ? (void *)f.tw_x64 : (void *)f.tw_x32));
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
@@ -467,8 +558,8 @@ int launch_rows(FftScratch &f, void *cube, const Geometry &g, const uint32_t *bi
 template <typename T, int LOGN, bool DB, bool RECUR>
 size_t cols_smem(int rpc) {
   constexpr int N = 1 << LOGN;
-  return fft_smem<T, LOGN>(rpc) * (DB ? 2 : 1) + (size_t)rpc * N * 8 +
-         (RECUR ? (size_t)rpc * N * 16 : 0);
+  return fft_smem<T, LOGN>(rpc) * (DB ? 2 : 1) + (RECUR ? (size_t)rpc * N * 16 : 0) +
+         2 * (size_t)(N / 32) * 4;
 }
 
 template <typename T, int LOGN, bool DB, bool RECUR>
@@ -502,29 +593,23 @@ int launch_cols(FftScratch &f, const void *cube, const Geometry &g, const double
                 const double *mtab, double wmin, double wmax, double norm, int phase_on,
                 double *img_re, double *img_im, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
-  constexpr bool RECUR = sizeof(T) == 4;  // mixed form
+  (void)cube;
+  // the per-pixel phase steps first, then the second column buffer, as they fit
   constexpr size_t kMax = 220 * 1024;
-  // double-buffer when two column buffers and the per-pixel tables fit
-  if (cols_smem<T, LOGN, true, RECUR>(BT / G) <= kMax)
-    return launch_cols_impl<T, LOGN, true, RECUR>(f, cube, g, ltab, mtab, wmin, wmax, norm,
+  if (cols_smem<T, LOGN, true, true>(BT / G) <= kMax)
+    return launch_cols_impl<T, LOGN, true, true>(f, cube, g, ltab, mtab, wmin, wmax, norm,
+                                                 phase_on, img_re, img_im, st);
+  if (cols_smem<T, LOGN, false, true>(BT / G) <= kMax)
+    return launch_cols_impl<T, LOGN, false, true>(f, cube, g, ltab, mtab, wmin, wmax, norm,
                                                   phase_on, img_re, img_im, st);
-  if (cols_smem<T, LOGN, false, RECUR>(BT / G) <= kMax)
-    return launch_cols_impl<T, LOGN, false, RECUR>(f, cube, g, ltab, mtab, wmin, wmax, norm,
-                                                   phase_on, img_re, img_im, st);
   return launch_cols_impl<T, LOGN, false, false>(f, cube, g, ltab, mtab, wmin, wmax, norm,
                                                  phase_on, img_re, img_im, st);
-}
-
-int ilog2(int n) {
-  int l = 0;
-  while ((1 << l) < n) l++;
-  return l;
 }
 
 }  // namespace
 
 bool sparse_fft_supported(int nx, int ny) {
-  // power-of-two axes; nx >= 64 also makes nx a multiple of the column block
+  // power-of-two axes from 64 to 8192 (nx >= 64 makes it a multiple of the tile)
   auto ok = [](int n) { return n >= 64 && n <= 8192 && (n & (n - 1)) == 0; };
   return ok(nx) && ok(ny);
 }
@@ -568,17 +653,17 @@ int sparse_row_list(FftScratch &f, const Geometry &g, cudaStream_t st) {
 #define RICK_FFT_SIZES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
 int sparse_fft_rows(int precision, FftScratch &f, void *cube, const Geometry &g,
-                    const uint32_t *bin_off, cudaStream_t st) {
+                    cudaStream_t st) {
   const int lx = ilog2(g.nx);
   if (precision == RICK_PREC_FP64) {
     switch (lx) {
-#define X(L) case L: return launch_rows<double, L>(f, cube, g, bin_off, st);
+#define X(L) case L: return launch_rows<double, L>(f, cube, g, st);
       RICK_FFT_SIZES(X)
 #undef X
     }
   } else {
     switch (lx) {
-#define X(L) case L: return launch_rows<float, L>(f, cube, g, bin_off, st);
+#define X(L) case L: return launch_rows<float, L>(f, cube, g, st);
       RICK_FFT_SIZES(X)
 #undef X
     }

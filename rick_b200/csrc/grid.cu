@@ -35,7 +35,8 @@ __global__ void __launch_bounds__(kGridThreads)
                  const uint32_t *__restrict__ item_off, uint32_t nbins, uint32_t max_chunk,
                  Geometry g, int kernel, const double *__restrict__ table, int accumulate,
                  uint64_t *__restrict__ counters,
-                 typename Vec2<OutT>::type *__restrict__ cube, uint32_t *__restrict__ rowmask) {
+                 typename Vec2<OutT>::type *__restrict__ cube, uint32_t *__restrict__ rowmask,
+                 uint32_t *__restrict__ tilemask) {
   __shared__ double s_re[kTile * kPitch];
   __shared__ double s_im[kTile * kPitch];
   __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
@@ -139,7 +140,11 @@ __global__ void __launch_bounds__(kGridThreads)
     __syncthreads();
 
     // Flush the tile (and the rows it touched).
-    if (rowmask && threadIdx.x == 0 && s_rows) atomicOr(&rowmask[(uint64_t)w * g.nty + ty], s_rows);
+    if (rowmask && threadIdx.x == 0 && s_rows) {
+      atomicOr(&rowmask[(uint64_t)w * g.nty + ty], s_rows);
+      const int tmw = (g.ntx + 31) / 32;
+      atomicOr(&tilemask[((uint64_t)w * g.nty + ty) * tmw + (tx >> 5)], 1u << (tx & 31));
+    }
     const uint64_t plane = (uint64_t)g.nx * g.ny;
     for (int c = threadIdx.x; c < kTile * kTile; c += blockDim.x) {
       const int y = c / kTile, x = c % kTile;
@@ -196,7 +201,7 @@ __global__ void k_zero_split_tiles(const uint32_t *__restrict__ item_off, uint32
 
 template <typename OutT>
 int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accumulate,
-                uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask) {
+                uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask, uint32_t *tilemask) {
   const int sms = num_sms();
   using V = typename Vec2<OutT>::type;
   const uint32_t nbins = (uint32_t)g.nbins();
@@ -207,12 +212,12 @@ int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accum
     k_grid_tiles<OutT, 8><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
                                                            nbins, max_chunk, g, kernel, s.table,
                                                            accumulate, s.counters, (V *)cube,
-                                                           rowmask);
+                                                           rowmask, tilemask);
   else
     k_grid_tiles<OutT, 16><<<blocks, kGridThreads, 0, st>>>(s.records, s.bin_count, s.item_off,
                                                             nbins, max_chunk, g, kernel, s.table,
                                                             accumulate, s.counters, (V *)cube,
-                                                            rowmask);
+                                                            rowmask, tilemask);
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
@@ -220,10 +225,11 @@ int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accum
 }  // namespace
 
 int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
-               int accumulate, uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask) {
+               int accumulate, uint32_t max_chunk, cudaStream_t st, uint32_t *rowmask,
+               uint32_t *tilemask) {
   if (precision == RICK_PREC_FP64)
-    return launch_grid<double>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask);
-  return launch_grid<float>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask);
+    return launch_grid<double>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask, tilemask);
+  return launch_grid<float>(g, kernel, s, cube, accumulate, max_chunk, st, rowmask, tilemask);
 }
 
 int zero_split_tiles(const Geometry &g, int precision, Scratch &s, void *cube, cudaStream_t st) {

@@ -298,13 +298,15 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
     // only the tiles several work items add into are cleared; the row mask
     // records which grid rows the footprints reach
     RICK_CUDA(cudaMemsetAsync(p->f.rowmask, 0, (size_t)p->g.nw * p->g.nty * 4, st));
+    RICK_CUDA(cudaMemsetAsync(p->f.tilemask, 0,
+                              (size_t)p->g.nw * p->g.nty * ((p->g.ntx + 31) / 32) * 4, st));
     RICK_TRY(zero_split_tiles(p->g, p->d.precision, p->s, p->cube, st));
   } else if (!accumulate) {
     RICK_CUDA(cudaMemsetAsync(p->cube, 0, p->cube_vals * p->val_bytes, st));
   }
   RICK_TRY(mark(p, p->ev[3], st));
   RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, chunk, st,
-                      sparse ? p->f.rowmask : nullptr));
+                      sparse ? p->f.rowmask : nullptr, sparse ? p->f.tilemask : nullptr));
   RICK_TRY(mark(p, p->ev[4], st));
   p->ran[0] = p->ran[1] = p->ran[3] = true;
   p->ran[2] = !accumulate;
@@ -322,7 +324,7 @@ int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const doub
                           1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, st, true));
   RICK_TRY(mark(p, p->ev_fft0, st));
   RICK_TRY(sparse_row_list(p->f, p->g, st));
-  RICK_TRY(sparse_fft_rows(p->d.precision, p->f, p->cube, p->g, p->s.bin_count, st));
+  RICK_TRY(sparse_fft_rows(p->d.precision, p->f, p->cube, p->g, st));
   RICK_TRY(mark(p, p->ev[5], st));
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
   RICK_TRY(ensure_lm(p, nx, ny, nx, ny, resolution, st));
@@ -450,6 +452,7 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
     A((void **)&p->f.rowmask, (size_t)desc->num_w_planes * p->g.nty * 4);
     A((void **)&p->f.rowlist, (size_t)desc->num_w_planes * ny * 4);
     A((void **)&p->f.counts, (size_t)(1 + desc->num_w_planes) * 4);
+    A((void **)&p->f.tilemask, (size_t)desc->num_w_planes * p->g.nty * ((p->g.ntx + 31) / 32) * 4);
     A((void **)&p->f.tw_x64, (size_t)nx * sizeof(double2));
     A((void **)&p->f.tw_y64, (size_t)ny * sizeof(double2));
     A((void **)&p->f.tw_x32, (size_t)nx * sizeof(float2));
@@ -491,7 +494,8 @@ int rick_plan_destroy(rick_plan *p) {
   void *ptrs[] = {p->cube, p->s.bin_count, p->s.bin_cursor, p->s.item_off, p->s.scan_tmp,
                   p->s.counters, p->s.records, p->s.table, p->d_lm, p->fft_work, p->h_rows_d,
                   p->d_img, p->d_stage, p->f.rowmask, p->f.rowlist, p->f.counts,
-                  p->f.tw_x64, p->f.tw_y64, p->f.tw_x32, p->f.tw_y32, p->f.blocked};
+                  p->f.tw_x64, p->f.tw_y64, p->f.tw_x32, p->f.tw_y32, p->f.blocked,
+                  p->f.tilemask};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->h_lm) cudaFreeHost(p->h_lm);

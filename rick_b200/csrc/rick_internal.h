@@ -86,7 +86,8 @@ struct Scratch {
 struct FftScratch {
   uint32_t *rowmask = nullptr;  // [nw * nty] bit k%32 of word (w, k/32): row k touched
   uint32_t *rowlist = nullptr;  // [nw * ny] touched (plane, row) ids
-  uint32_t *counts = nullptr;   // [1 + nw] total touched rows, then per plane
+  uint32_t *counts = nullptr;   // [1 + nw] touched rows, then touched rows per plane
+  uint32_t *tilemask = nullptr; // [nw * nty * ceil(ntx/32)] bit tx: tile (w, ty, tx) holds records
   double2 *tw_x64 = nullptr, *tw_y64 = nullptr;  // per-pass twiddles of the two axes
   float2 *tw_x32 = nullptr, *tw_y32 = nullptr;
   void *blocked = nullptr;      // row-transformed planes, column-blocked (cube-sized)
@@ -112,7 +113,7 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
              uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid = nullptr);
 int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
                int accumulate, uint32_t max_chunk, cudaStream_t st,
-               uint32_t *rowmask = nullptr);
+               uint32_t *rowmask = nullptr, uint32_t *tilemask = nullptr);
 // Zeroes the tiles that several work items add into (the sparse path does not
 // clear the cube).
 int zero_split_tiles(const Geometry &g, int precision, Scratch &s, void *cube, cudaStream_t st);
@@ -121,7 +122,7 @@ bool sparse_fft_supported(int nx, int ny);
 void make_twiddles(int n, double2 *t64, float2 *t32);
 int sparse_row_list(FftScratch &f, const Geometry &g, cudaStream_t st);
 int sparse_fft_rows(int precision, FftScratch &f, void *cube, const Geometry &g,
-                    const uint32_t *bin_off, cudaStream_t st);
+                    cudaStream_t st);
 int sparse_fft_cols_image(int precision, FftScratch &f, const void *cube, const Geometry &g,
                           const double *ltab, const double *mtab, double wmin, double wmax,
                           double norm, int phase_on, double *img_re, double *img_im,
