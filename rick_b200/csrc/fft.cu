@@ -262,6 +262,124 @@ __device__ __forceinline__ void fft_to_regs(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
+// PP transforms at once, one per shared buffer, sharing every barrier (twice
+// the independent work between barriers for PP = 2).
+template <typename T, int N, int R, int PP>
+__device__ __forceinline__ void stockham_pass_pp(typename V2<T>::t *const *s, int t, int Ns,
+                                                 const typename V2<T>::t *__restrict__ tw) {
+  constexpr int G = N / kVpt, B = kVpt / R;
+  Cx<T> v[PP][B][R];
+#pragma unroll
+  for (int pp = 0; pp < PP; pp++)
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int j = t + b * G;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[pp][b][r] = lds<T>(s[pp], j + r * (N / R));
+    }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * G;
+    const int jm = j & (Ns - 1);
+    Cx<T> w[R];
+    w[0] = {(T)1, (T)0};
+    if (Ns > 1) {
+      const typename V2<T>::t *twp = tw + (Ns - 1) + jm;
+      if (R == 8) {
+        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
+        w[1] = {a.x, a.y};
+        w[2] = {b2.x, b2.y};
+        w[4] = {b4.x, b4.y};
+        w[3] = cmul<T>(w[1], w[2].re, w[2].im);
+        w[5] = cmul<T>(w[1], w[4].re, w[4].im);
+        w[6] = cmul<T>(w[2], w[4].re, w[4].im);
+        w[7] = cmul<T>(w[3], w[4].re, w[4].im);
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+          const typename V2<T>::t a = __ldg(twp + (r - 1) * Ns);
+          w[r] = {a.x, a.y};
+        }
+      }
+    }
+    const int idx = (j - jm) * R + jm;
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) {
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; r++) v[pp][b][r] = cmul<T>(v[pp][b][r], w[r].re, w[r].im);
+      }
+      Dft<T, R>::run(v[pp][b]);
+#pragma unroll
+      for (int r = 0; r < R; r++) sts<T>(s[pp], idx + r * Ns, v[pp][b][r]);
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T, int N, int R, int PP>
+__device__ __forceinline__ void stockham_last_pass_pp(typename V2<T>::t *const *s, int t,
+                                                      const typename V2<T>::t *__restrict__ tw,
+                                                      Cx<T> out[PP][kVpt]) {
+  constexpr int G = N / kVpt, B = kVpt / R, Ns = N / R;
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * G;  // j < Ns: the output index is j + r*Ns
+    Cx<T> w[R];
+    w[0] = {(T)1, (T)0};
+    if (Ns > 1) {
+      const typename V2<T>::t *twp = tw + (Ns - 1) + j;
+      if (R == 8) {
+        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
+        w[1] = {a.x, a.y};
+        w[2] = {b2.x, b2.y};
+        w[4] = {b4.x, b4.y};
+        w[3] = cmul<T>(w[1], w[2].re, w[2].im);
+        w[5] = cmul<T>(w[1], w[4].re, w[4].im);
+        w[6] = cmul<T>(w[2], w[4].re, w[4].im);
+        w[7] = cmul<T>(w[3], w[4].re, w[4].im);
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+          const typename V2<T>::t a = __ldg(twp + (r - 1) * Ns);
+          w[r] = {a.x, a.y};
+        }
+      }
+    }
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) {
+      Cx<T> v[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) v[r] = lds<T>(s[pp], j + r * (N / R));
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; r++) v[r] = cmul<T>(v[r], w[r].re, w[r].im);
+      }
+      Dft<T, R>::run(v);
+#pragma unroll
+      for (int r = 0; r < R; r++) out[pp][b + B * r] = v[r];
+    }
+  }
+}
+
+template <typename T, int LOGN, int PP>
+__device__ __forceinline__ void fft_to_regs_pp(typename V2<T>::t *const *s, int t,
+                                               const typename V2<T>::t *__restrict__ tw,
+                                               Cx<T> out[PP][kVpt]) {
+  constexpr int N = 1 << LOGN;
+  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+  constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
+  constexpr int NPASS = P8 + (REM ? 1 : 0);
+  int Ns = 1;
+#pragma unroll
+  for (int p = 0; p < NPASS - 1; p++) {
+    stockham_pass_pp<T, N, 8, PP>(s, t, Ns, tw);
+    Ns *= 8;
+  }
+  stockham_last_pass_pp<T, N, LASTR, PP>(s, t, tw, out);
+}
+
 // Whole inverse FFT of N = 2^LOGN points (unnormalised), in place.
 template <typename T, int LOGN>
 __device__ __forceinline__ void fft_inplace(typename V2<T>::t *s, int t,
@@ -354,7 +472,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
 // less than the rounding of the reference's own argument (~3e-13).
 constexpr int kAnchor = 8;
 
-template <typename T, int LOGN, bool DB, bool RECUR>
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __global__ void __launch_bounds__(block_threads<LOGN>())
     k_fft_cols_image(const typename V2<T>::t *__restrict__ cube, int nx, int ny, int nw, int nty,
                      const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts,
@@ -363,15 +481,16 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
                      double norm, int phase_on, double *__restrict__ img_re,
                      double *__restrict__ img_im) {
   constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  constexpr int NB = (DB ? 2 : 1) * PP;  // column buffers per row group
   using V = typename V2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *s = reinterpret_cast<V *>(smem_raw);
   const int rpc = blockDim.x / G;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
-  V *buf[2] = {s + grp * LEN, s + (DB ? rpc + grp : grp) * LEN};
-  double2 *tables = reinterpret_cast<double2 *>(s + (DB ? 2 : 1) * rpc * LEN);
+  V *sbase = s + grp * NB * LEN;  // buffers [set][pp]: set = cur (DB), pp < PP
+  double2 *tables = reinterpret_cast<double2 *>(s + rpc * NB * LEN);
   double2 *sstep = tables + grp * N;  // RECUR only
-  // row masks of the next two planes to load (the CTA's columns share them)
+  // row masks of the planes of the next two sets (2 * PP slots)
   uint32_t *smask = reinterpret_cast<uint32_t *>(tables + (RECUR ? rpc * N : 0));
   const bool phase = phase_on && nw > 1;
   const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
@@ -379,27 +498,42 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
     do { iw++; } while (iw < nw && counts[1 + iw] == 0);  // planes without data add exact zeros
     return iw;
   };
-  auto stage_mask = [&](int slot, int iw) {
-    if (iw < nw)
-      for (int i = threadIdx.x; i < nty; i += blockDim.x)
-        smask[slot * nty + i] = rowmask[(uint64_t)iw * nty + i];
-  };
-  auto load_column = [&](V *dst, int iw, int slot, uint32_t n, bool active) {
-    const uint32_t *mask = smask + slot * nty;
-    constexpr int CB = col_block<T>();
-    const V *col = cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);  // row k at k * CB
+  // the next PP planes with data after plane `after` (nw = none)
+  auto next_set = [&](int after, int set[PP]) {
 #pragma unroll
-    for (int q = 0; q < kVpt; q++) {
-      const int k = t + q * G;
-      const bool touched = active && ((mask[k >> 5] >> (k & 31)) & 1u);
-      if (DB) {
-        cp_async_zfill<T>(dst + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
-      } else {
-        V v;
-        v.x = 0;
-        v.y = 0;
-        if (touched) v = col[(uint64_t)k * CB];
-        dst[pad(k)] = v;
+    for (int pp = 0; pp < PP; pp++) {
+      after = next_plane(after);
+      set[pp] = after;
+      if (after >= nw) after = nw;
+    }
+  };
+  auto stage_masks = [&](int slot, const int set[PP]) {
+    for (int i = threadIdx.x; i < PP * nty; i += blockDim.x) {
+      const int pp = i / nty, word = i % nty;
+      if (set[pp] < nw) smask[(slot * PP + pp) * nty + word] = rowmask[(uint64_t)set[pp] * nty + word];
+    }
+  };
+  auto load_set = [&](int bset, const int set[PP], int slot, uint32_t n, bool active) {
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) {
+      if (set[pp] >= nw) continue;
+      V *dst = sbase + (bset * PP + pp) * LEN;
+      const uint32_t *mask = smask + (slot * PP + pp) * nty;
+      constexpr int CB = col_block<T>();
+      const V *col = cube + blocked_index<T>(set[pp], 0, active ? n : 0, nx, ny);
+#pragma unroll
+      for (int q = 0; q < kVpt; q++) {
+        const int k = t + q * G;
+        const bool touched = active && ((mask[k >> 5] >> (k & 31)) & 1u);
+        if (DB) {
+          cp_async_zfill<T>(dst + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
+        } else {
+          V v;
+          v.x = 0;
+          v.y = 0;
+          if (touched) v = col[(uint64_t)k * CB];
+          dst[pad(k)] = v;
+        }
       }
     }
   };
@@ -416,10 +550,11 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
     double acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
 #pragma unroll
     for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = 0.0;
-    int iw = next_plane(-1);
-    int nxt = next_plane(iw);
-    stage_mask(0, iw);
-    stage_mask(1, nxt);
+    int cur[PP], nxt[PP];
+    next_set(-1, cur);
+    next_set(cur[PP - 1], nxt);
+    stage_masks(0, cur);
+    stage_masks(1, nxt);
     if (phase && RECUR) {
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
@@ -430,69 +565,82 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
       }
     }
     __syncthreads();
-    if (DB && iw < nw) {
-      load_column(buf[0], iw, 0, n, active);
+    if (DB && cur[0] < nw) {
+      load_set(0, cur, 0, n, active);
       cp_async_commit();
     }
-    int cur = 0, it = 0;
+    int bset = 0, it = 0;
     int last_anchor = -kAnchor, prev_iw = -1;
-    while (iw < nw) {
-      const int nn = next_plane(nxt);  // plane after the next one
+    while (cur[0] < nw) {
+      int nn[PP];
+      next_set(nxt[PP - 1], nn);  // the set after the next one
       if (DB) {
-        if (nxt < nw) load_column(buf[cur ^ 1], nxt, (it + 1) & 1, n, active);
+        if (nxt[0] < nw) load_set(bset ^ 1, nxt, (it + 1) & 1, n, active);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
-        load_column(buf[0], iw, it & 1, n, active);
+        load_set(0, cur, it & 1, n, active);
       }
       __syncthreads();
-      // this plane's mask slot is free now: stage the plane after next
-      stage_mask(it & 1, nn);
-      Cx<T> x[kVpt];
-      fft_to_regs<T, LOGN>(buf[cur], t, tw, x);
-      const bool anchor = !RECUR || iw - last_anchor >= kAnchor;
-      const int gap = iw - prev_iw;  // planes since the previous factor (empty planes skipped)
-      double cw = 0.0;
-      if (anchor) {
-        last_anchor = iw;
-        cw = __dmul_rn(twopi, __dadd_rn(wmin, __dmul_rn((double)iw, dw)));  // 2 pi wterm
-      }
-      prev_iw = iw;
+      // this set's mask slot is free now: stage the set after next
+      stage_masks(it & 1, nn);
+      V *bufs[PP];
 #pragma unroll
-      for (int q = 0; q < kVpt; q++) {
-        const int m = t + q * G;
-        const double p = __dmul_rn(norm, (double)x[q].re), qq = __dmul_rn(norm, (double)x[q].im);
-        if (phase) {
-          if (anchor) {
-            const double root = root_of(l, m);
-            double sn, cs;
-            sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
-            const double amp = dwnorm * root;
-            ph_re[q] = cs * amp;
-            ph_im[q] = sn * amp;
-          } else {
-            const double2 st = sstep[m];
-            double sr = st.x, si = st.y;
-            for (int g2 = 1; g2 < gap; g2++) {
-              const double tr = sr * st.x - si * st.y;
-              si = sr * st.y + si * st.x;
-              sr = tr;
+      for (int pp = 0; pp < PP; pp++) bufs[pp] = sbase + ((DB ? bset : 0) * PP + pp) * LEN;
+      Cx<T> x[PP][kVpt];
+      fft_to_regs_pp<T, LOGN, PP>(bufs, t, tw, x);
+#pragma unroll
+      for (int pp = 0; pp < PP; pp++) {
+        const int iw = cur[pp];
+        if (iw >= nw) break;
+        const bool anchor = !RECUR || iw - last_anchor >= kAnchor;
+        const int gap = iw - prev_iw;  // planes since the previous factor (empty planes skipped)
+        double cw = 0.0;
+        if (anchor) {
+          last_anchor = iw;
+          cw = __dmul_rn(twopi, __dadd_rn(wmin, __dmul_rn((double)iw, dw)));  // 2 pi wterm
+        }
+        prev_iw = iw;
+#pragma unroll
+        for (int q = 0; q < kVpt; q++) {
+          const int m = t + q * G;
+          const double p = __dmul_rn(norm, (double)x[pp][q].re);
+          const double qq = __dmul_rn(norm, (double)x[pp][q].im);
+          if (phase) {
+            if (anchor) {
+              const double root = root_of(l, m);
+              double sn, cs;
+              sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+              const double amp = dwnorm * root;
+              ph_re[q] = cs * amp;
+              ph_im[q] = sn * amp;
+            } else {
+              const double2 st = sstep[m];
+              double sr = st.x, si = st.y;
+              for (int g2 = 1; g2 < gap; g2++) {
+                const double tr = sr * st.x - si * st.y;
+                si = sr * st.y + si * st.x;
+                sr = tr;
+              }
+              const double tr = ph_re[q] * sr - ph_im[q] * si;
+              ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
+              ph_re[q] = tr;
             }
-            const double tr = ph_re[q] * sr - ph_im[q] * si;
-            ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
-            ph_re[q] = tr;
+            acc_re[q] += p * ph_re[q] - qq * ph_im[q];
+            acc_im[q] += p * ph_im[q] + qq * ph_re[q];
+          } else {
+            acc_re[q] += p;
+            acc_im[q] += qq;
           }
-          acc_re[q] += p * ph_re[q] - qq * ph_im[q];
-          acc_im[q] += p * ph_im[q] + qq * ph_re[q];
-        } else {
-          acc_re[q] += p;
-          acc_im[q] += qq;
         }
       }
       __syncthreads();
-      if (DB) cur ^= 1;
-      iw = nxt;
-      nxt = nn;
+      if (DB) bset ^= 1;
+#pragma unroll
+      for (int pp = 0; pp < PP; pp++) {
+        cur[pp] = nxt[pp];
+        nxt[pp] = nn[pp];
+      }
       it++;
     }
     if (DB) cp_async_wait<0>();
@@ -555,32 +703,32 @@ int launch_rows(FftScratch &f, void *cube, const Geometry &g, cudaStream_t st) {
   return RICK_OK;
 }
 
-template <typename T, int LOGN, bool DB, bool RECUR>
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 size_t cols_smem(int rpc) {
   constexpr int N = 1 << LOGN;
-  return fft_smem<T, LOGN>(rpc) * (DB ? 2 : 1) + (RECUR ? (size_t)rpc * N * 16 : 0) +
-         2 * (size_t)(N / 32) * 4;
+  return fft_smem<T, LOGN>(rpc) * (DB ? 2 : 1) * PP + (RECUR ? (size_t)rpc * N * 16 : 0) +
+         2 * PP * (size_t)(N / 32) * 4;
 }
 
-template <typename T, int LOGN, bool DB, bool RECUR>
-int launch_cols_impl(FftScratch &f, const void *cube, const Geometry &g, const double *ltab,
-                     const double *mtab, double wmin, double wmax, double norm, int phase_on,
-                     double *img_re, double *img_im, cudaStream_t st) {
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
+int launch_cols_impl(FftScratch &f, const Geometry &g, const double *ltab, const double *mtab,
+                     double wmin, double wmax, double norm, int phase_on, double *img_re,
+                     double *img_im, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
   const int rpc = BT / G;
-  const size_t sm = cols_smem<T, LOGN, DB, RECUR>(rpc);
-  RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_image<T, LOGN, DB, RECUR>,
+  const size_t sm = cols_smem<T, LOGN, DB, RECUR, PP>(rpc);
+  RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_image<T, LOGN, DB, RECUR, PP>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int per_sm = 0;
   RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, k_fft_cols_image<T, LOGN, DB, RECUR>, BT, sm));
+      &per_sm, k_fft_cols_image<T, LOGN, DB, RECUR, PP>, BT, sm));
   const int want = (g.nx + rpc - 1) / rpc;
   const int blocks = std::min(want, num_sms() * std::max(per_sm, 1));
   // phase_correction.cu:100-102
   const double dw = (wmax - wmin) / (double)g.nw;
   const double dwnorm = dw / (wmax - wmin);
   RICK_LAUNCHED();
-  k_fft_cols_image<T, LOGN, DB, RECUR><<<blocks, BT, sm, st>>>(
+  k_fft_cols_image<T, LOGN, DB, RECUR, PP><<<blocks, BT, sm, st>>>(
       (const typename V2<T>::t *)f.blocked, g.nx, g.ny, g.nw, g.nty, f.rowmask, f.counts,
       (const typename V2<T>::t *)(sizeof(T) == 8 ? (void *)f.tw_y64 : (void *)f.tw_y32), ltab,
       mtab, wmin, dw, dwnorm, norm, phase_on, img_re, img_im);
@@ -593,17 +741,23 @@ int launch_cols(FftScratch &f, const void *cube, const Geometry &g, const double
                 const double *mtab, double wmin, double wmax, double norm, int phase_on,
                 double *img_re, double *img_im, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
+  constexpr int rpc = BT / G;
   (void)cube;
-  // the per-pixel phase steps first, then the second column buffer, as they fit
+  // in order of preference, the first that fits: two planes per iteration
+  // (FP32), double-buffered loads, the per-pixel phase steps
   constexpr size_t kMax = 220 * 1024;
-  if (cols_smem<T, LOGN, true, true>(BT / G) <= kMax)
-    return launch_cols_impl<T, LOGN, true, true>(f, cube, g, ltab, mtab, wmin, wmax, norm,
-                                                 phase_on, img_re, img_im, st);
-  if (cols_smem<T, LOGN, false, true>(BT / G) <= kMax)
-    return launch_cols_impl<T, LOGN, false, true>(f, cube, g, ltab, mtab, wmin, wmax, norm,
-                                                  phase_on, img_re, img_im, st);
-  return launch_cols_impl<T, LOGN, false, false>(f, cube, g, ltab, mtab, wmin, wmax, norm,
-                                                 phase_on, img_re, img_im, st);
+#define RICK_TRY_COLS(DB, RC, PP)                                                              \
+  if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)                                             \
+    return launch_cols_impl<T, LOGN, DB, RC, PP>(f, g, ltab, mtab, wmin, wmax, norm, phase_on, \
+                                                 img_re, img_im, st);
+  if constexpr (sizeof(T) == 4) {
+    RICK_TRY_COLS(true, true, 2)
+  }
+  RICK_TRY_COLS(true, true, 1)
+  RICK_TRY_COLS(false, true, 1)
+#undef RICK_TRY_COLS
+  return launch_cols_impl<T, LOGN, false, false, 1>(f, g, ltab, mtab, wmin, wmax, norm, phase_on,
+                                                    img_re, img_im, st);
 }
 
 }  // namespace
