@@ -43,9 +43,15 @@ sys.path.insert(0, ROOT)
 METRIC = "imaged vis/s (1xB200) FP32-mixed vs FP64 plain @<=1e-5 rel err; p50/p99 lat"
 WORKLOAD = dict(name="c2", grid=4096, w_planes=32, kernel="kaiser_bessel", w_support=7)
 
-# DRAM traffic per launch measured by ncu for the dominant kernels (bytes),
-# scaled to the full workload (profiles/ summaries give the captures).
-NCU_TRAFFIC = {}
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that ncu
+# measured for each stage's kernel on this workload at full size (FP64 form, one
+# metric pass; profiles/traffic_c2.md has the command and the read/write split).
+NCU_TRAFFIC = {"bin_count": 125_663_488, "bin_scatter": 10_906_619_904,
+               "grid": 386_896_128, "fft": 2_084_043_264, "phase": 2_399_146_496}
+# the kernel behind each plan stage on the sparse-aware path (FP64, 4096^2)
+STAGE_KERNELS = {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
+                 "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
+                 "fft": "k_fft_rows<double,12>", "phase": "k_fft_cols_image<double,12,1,1,1>"}
 
 
 def parse():
@@ -129,11 +135,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(n_rows, nvis, npol, records, nx, ny, nw, val_bytes):
-    """Per-stage algorithmic bytes (the minimum each stage must move)."""
+def algorithmic_bytes(n_rows, nvis, npol, records, nx, ny, nw, val_bytes, fft_rows=0):
+    """Per-stage algorithmic bytes (the minimum each stage must move).
+
+    With the sparse-aware FFT (fft_rows > 0: the (plane, row) pairs the gridder
+    touched) the row pass reads those rows of the cube and writes them to the
+    column-blocked buffer, and the column pass reads them back once and writes
+    the FP64 image; the cube is not cleared (stage cube_zero only clears the
+    row/tile masks and the split tiles)."""
     g = 2 * nw * nx * ny * val_bytes                 # the cube
     rec = 40 * records                                # binned row records
-    return {
+    out = {
         "bin_count": 24 * n_rows,                                   # u,v,w read once
         "bin_scatter": 8 * nvis + n_rows * (24 + 4 * npol) + rec,   # vis+uvw+weights in, records out
         "cube_zero": g,
@@ -141,6 +153,10 @@ def algorithmic_bytes(n_rows, nvis, npol, records, nx, ny, nw, val_bytes):
         "fft": 2 * g,                                               # one read + one write
         "phase": g + 16 * nx * ny,                                  # cube in, FP64 image out
     }
+    if fft_rows:
+        touched = fft_rows * nx * 2 * val_bytes
+        out.update({"cube_zero": 0, "fft": 2 * touched, "phase": touched + 16 * nx * ny})
+    return out
 
 
 def run_ours(args):
@@ -266,17 +282,24 @@ def run_ours(args):
         del host
 
     hbm, peak_kind = peaks()
-    alg = algorithmic_bytes(n, nvis, npol, stats64["records"], nx, ny, nw, 8)
+    alg = algorithmic_bytes(n, nvis, npol, stats64["records"], nx, ny, nw, 8,
+                            stats64.get("fft_rows", 0))
     dom = max(stage64, key=stage64.get)
     achieved = alg[dom] / (stage64[dom] * 1e-3) / 1e9
-    roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1),
+    roofline = {"kernel": dom, "kernel_name": STAGE_KERNELS.get(dom, dom),
+                "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "traffic": NCU_TRAFFIC.get(dom), "peak_source": peak_kind,
                 "algorithmic_bytes": alg[dom],
                 "stages_ms": {k: round(v, 4) for k, v in stage64.items()},
                 "stages_frac": {k: round(alg[k] / (v * 1e-3) / 1e9 / hbm, 4)
-                                for k, v in stage64.items() if v > 0}}
+                                for k, v in stage64.items() if v > 0 and alg[k] > 0},
+                "fft_rows": stats64.get("fft_rows", 0)}
+    if dom == "phase" and stats64.get("fft_rows", 0):
+        roofline["note"] = ("column FFT + w-correction + plane sum: bound by FP64 issue and "
+                            "latency (one 4096-point column of 16 warps per SM), not by HBM")
     g8 = 2 * nw * nx * ny * 8
+    in_bytes = sum(int(r.numel() * r.element_size()) for r in rows)
     pipe_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -289,7 +312,8 @@ def run_ours(args):
                                "(1.305e9 vis), 4096^2 x 32 w-planes, Kaiser-Bessel support 7",
                    "rows": n, "visibilities": nvis, "grid": nx, "w_planes": nw,
                    "kernel": cfg.kernel, "w_support": cfg.w_support,
-                   "l2": "inputs (10.6 GB) larger than L2; no flush",
+                   "l2": f"inputs ({in_bytes / 1e9:.2f} GB) larger than L2; no flush"
+                         if in_bytes > 126e6 else "inputs smaller than L2",
                    "parallelism": f"replicas x{world}", "time_fraction": args.time_fraction},
         "e2e": e2e, "gpu_launches": launches,
         "roofline": roofline,

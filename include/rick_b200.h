@@ -122,6 +122,8 @@ typedef struct rick_plan_stats {
   uint64_t records;        /* binned row records (rows touching k tiles count k) */
   uint64_t work_items;     /* gridder work items (tile chunks) */
   uint64_t device_bytes;   /* HBM held by the plan */
+  uint64_t fft_rows;       /* (plane, row) pairs the last rick_plan_image transformed on its
+                              sparse path (rows the gridder touched); 0 after the dense path */
 } rick_plan_stats;
 
 /* Row selection applied by the gridding calls. */

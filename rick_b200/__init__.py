@@ -57,7 +57,8 @@ class PlanDesc(C.Structure):
 class PlanStats(C.Structure):
     _fields_ = [("rows_in", C.c_uint64), ("rows_gridded", C.c_uint64),
                 ("rows_dropped", C.c_uint64), ("records", C.c_uint64),
-                ("work_items", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("work_items", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("fft_rows", C.c_uint64)]
 
 
 _lib = None

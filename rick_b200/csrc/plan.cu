@@ -705,6 +705,11 @@ int rick_plan_get_stats(rick_plan *p, rick_plan_stats *out) {
   RICK_CUDA(cudaMemcpy(&items, p->s.item_off + p->g.nbins(), 4, cudaMemcpyDeviceToHost));
   out->work_items = items;
   out->device_bytes = p->device_bytes;
+  if (p->cube_state == kCubeSparse) {
+    uint32_t rows = 0;
+    RICK_CUDA(cudaMemcpy(&rows, p->f.counts, 4, cudaMemcpyDeviceToHost));
+    out->fft_rows = rows;
+  }
   return RICK_OK;
 }
 
