@@ -68,6 +68,11 @@ def parse():
                     help="comma list of precision forms to time (fp64 first is the headline)")
     ap.add_argument("--grid", type=int, default=0, help="override the grid size (profiling cases)")
     ap.add_argument("--w-planes", type=int, default=0, help="override the w-planes (profiling)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-snapshot leg (256 small jobs, one graph)")
+    ap.add_argument("--jobs", type=int, default=256, help="jobs of the batched-snapshot leg")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run only the batched-snapshot leg and print its line (profiling)")
     return ap.parse_args()
 
 
@@ -335,12 +340,101 @@ def run_ours(args):
                 "generate_s": gen_s},
         "cpu_baseline": cpu,
     }
+    if not args.no_batched and world == 1:
+        line["batched"] = run_batched(args, dev, stream)
     if rank == 0:
         line["clocks"] = clocks.summary()
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_batched(args, dev, stream):
+    """Batched snapshot imaging: 256 independent ALMA-like jobs (visibility counts
+    log-uniform in 1e4-1e7, grids 256^2-2048^2, 4-16 w-planes, 1-4 channels,
+    2 polarisations), the mixed form as one autotuned batch replayed from its CUDA
+    graph, against every job imaged alone through a plan in the FP64 plain form."""
+    import torch
+    import rick_b200 as R
+    from rick_b200 import synth
+
+    t0 = time.time()
+    specs = synth.snapshot_jobs(args.jobs, device=str(dev))
+    torch.cuda.synchronize()
+    gen_s = time.time() - t0
+
+    def job_list(precision):
+        jobs, imgs = [], []
+        for sp in specs:
+            o, g = sp.obs, sp.grid
+            img = torch.empty(2 * g * g, dtype=torch.float64, device=dev)
+            geom = R.Geometry(g, g, sp.w_planes, sp.w_support, sp.kernel, precision)
+            rows = (o.uu, o.vv, o.ww, o.weights, o.vis_re, o.vis_im)
+            jobs.append(R.Job(geom, o.rows, o.cfg.nchan, o.cfg.npol, rows,
+                              R.resolution_of(o.meta), o.meta["wmin"], o.meta["wmax"],
+                              img[: g * g], img[g * g:]))
+            imgs.append(img)
+        return jobs, imgs
+
+    total_vis = sum(sp.nvis for sp in specs)
+    jobs, imgs = job_list("mixed")
+    t0 = time.time()
+    batch = R.Batch(jobs, "mixed", device=dev.index or 0)   # autotunes, captures the graph
+    create_s = time.time() - t0
+    for _ in range(args.warmup):
+        batch.run(stream)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.nvtx.range_push("batched_timed")
+    evs[0].record(stream)
+    for k in range(args.steps):
+        batch.run(stream)
+        evs[k + 1].record(stream)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    ms = evs[0].elapsed_time(evs[-1]) / args.steps
+    st = batch.stats()
+    tune = batch.tuning()
+    kernels = batch.kernels_per_run()
+    mixed_imgs = [im.clone() for im in imgs]
+    batch.close()
+    del imgs
+
+    # every job alone, FP64 plain form, one plan per job (created untimed)
+    alone_ms, errs = 0.0, []
+    for sp, (job, mimg) in zip(specs, zip(jobs, mixed_imgs)):
+        o, g = sp.obs, sp.grid
+        geom = R.Geometry(g, g, sp.w_planes, sp.w_support, sp.kernel, "fp64")
+        with R.Plan(geom, o.rows, o.cfg.nchan, o.cfg.npol, device=dev.index or 0) as plan:
+            img = torch.empty(2 * g * g, dtype=torch.float64, device=dev)
+            call = lambda: plan.image(o.rows, job.rows, job.resolution, job.wmin, job.wmax,
+                                      img[: g * g], img[g * g:], R.ROWS_ALL, stream)
+            call()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            alone_ms += e0.elapsed_time(e1)
+            den = torch.linalg.vector_norm(img)
+            errs.append(float(torch.linalg.vector_norm(mimg - img) / den) if den > 0 else 0.0)
+    return {"workload": f"{len(specs)} ALMA-like snapshot jobs, {total_vis:.3e} vis, grids "
+                        f"256^2-2048^2, 4-16 w-planes, Kaiser-Bessel support 7",
+            "visibilities": total_vis, "jobs": len(specs),
+            "grids": {str(g): sum(1 for sp in specs if sp.grid == g) for g in (256, 512, 1024, 2048)},
+            "mixed_batched": {"vis_per_s": total_vis / (ms * 1e-3), "ms_per_batch": ms,
+                              "p50_ms": float(np.percentile(per, 50)),
+                              "p99_ms": float(np.percentile(per, 99)),
+                              "gpu_launches_per_batch": kernels, "graph_launches_per_batch": 1,
+                              "tuning": tune,
+                              "create_s": create_s, "rows_gridded": st["rows_gridded"],
+                              "fft_rows": st["fft_rows"]},
+            "fp64_alone": {"vis_per_s": total_vis / (alone_ms * 1e-3), "ms_total": alone_ms},
+            "batched_mixed_over_fp64_alone": alone_ms / ms,
+            "rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "generate_s": gen_s}
 
 
 def _threads():
@@ -457,6 +551,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_batched:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps(run_batched(args, dev, torch.cuda.current_stream(dev))), flush=True)
     else:
         run_ours(args)
 

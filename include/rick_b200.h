@@ -133,7 +133,9 @@ typedef struct rick_plan_stats {
 
 int rick_plan_create(rick_plan **plan, const rick_plan_desc *desc);
 int rick_plan_destroy(rick_plan *plan);
-/* Bytes of HBM a plan with this description would hold (for admission). */
+/* Bytes of HBM a plan with this description would hold (for admission).  On
+ * power-of-two grids (the sparse-aware FFT of rick_plan_image) this excludes the
+ * cuFFT work area, which the stage call rick_plan_fft allocates on first use. */
 int rick_plan_footprint(const rick_plan_desc *desc, uint64_t *bytes);
 
 /* Grid device-resident rows into the plan's cube (overwrites the cube). */
@@ -200,6 +202,56 @@ int rick_wstack_noalloc(int num_w_planes, uint64_t num_points, uint32_t freq_per
                         int grid_size_x, int grid_size_y, double *grid, void *stream);
 int rick_wstack_noalloc_capacity(int num_w_planes, int grid_size_x, int grid_size_y,
                                  uint64_t *max_rows);
+
+/* ---- 4. Batched imaging -------------------------------------------------
+ * No counterpart in the reference (one rank images one dataset per run).  Many
+ * independent imaging jobs of uneven sizes -- each one rick_plan_image call:
+ * gridding, per-plane inverse FFT, w-correction and plane sum -- run as one
+ * launch per stage over all jobs, the stage sequence captured once in a CUDA
+ * graph.  Job inputs and images are device pointers that must stay valid
+ * while the batch exists; every run recomputes every image from the rows
+ * (images are overwritten).  Grid axes are powers of two in [64, 4096]. */
+#define RICK_BATCH_MAX_GRID 4096
+
+typedef struct rick_job_desc {
+  int grid_size_x, grid_size_y, num_w_planes, w_support, kernel;
+  uint64_t num_rows;
+  uint32_t freq_per_chan, polarizations;
+  int row_selection;   /* RICK_ROWS_ALL or RICK_ROWS_SECTOR0 */
+  int phase_on;        /* PHASE_ON of phase_correction.cu */
+  double resolution, wmin, wmax;
+  const double *uu, *vv, *ww;            /* device [num_rows], normalised */
+  const float *weight;                   /* device [num_rows * polarizations] */
+  const float *vis_real, *vis_img;       /* device [num_rows * freq_per_chan * polarizations] */
+  double *image_real, *image_imag;       /* device [grid_size_y * grid_size_x] */
+} rick_job_desc;
+
+/* Schedule knobs of a batch: gridder records per work item, gridder blocks per
+ * SM, and w-planes the column pass keeps in flight per iteration (1 or 2; 2 is
+ * used by the mixed form only). */
+typedef struct rick_batch_tuning {
+  uint32_t max_chunk;
+  int grid_blocks_per_sm;
+  int planes_in_flight;
+} rick_batch_tuning;
+
+typedef struct rick_batch rick_batch;
+
+/* HBM the batch holds (cubes, column-blocked planes, records, tables). */
+int rick_batch_footprint(const rick_job_desc *jobs, int njobs, int precision, uint64_t *bytes);
+/* Creates the batch on `device` (precision RICK_PREC_*).  tuning == NULL runs
+ * the autotuner (times candidate schedules on the batch itself, synchronises,
+ * writes the images; results cached per batch shape for the process). */
+int rick_batch_create(rick_batch **batch, const rick_job_desc *jobs, int njobs, int precision,
+                      int device, const rick_batch_tuning *tuning);
+/* One graph launch on `stream` (a cudaStream_t); asynchronous. */
+int rick_batch_run(rick_batch *batch, void *stream);
+int rick_batch_get_tuning(rick_batch *batch, rick_batch_tuning *tuning);
+/* Kernel launches one run replays from the graph (all jobs together). */
+int rick_batch_kernels_per_run(rick_batch *batch, uint32_t *kernels);
+/* Totals over all jobs of the last run (synchronises). */
+int rick_batch_get_stats(rick_batch *batch, rick_plan_stats *stats);
+int rick_batch_destroy(rick_batch *batch);
 
 /* Names of the kernels this library launches, and how many launches it has
  * issued in this process (for launch accounting). */

@@ -61,6 +61,22 @@ class PlanStats(C.Structure):
                 ("fft_rows", C.c_uint64)]
 
 
+class JobDesc(C.Structure):
+    _fields_ = [("grid_size_x", C.c_int), ("grid_size_y", C.c_int), ("num_w_planes", C.c_int),
+                ("w_support", C.c_int), ("kernel", C.c_int), ("num_rows", C.c_uint64),
+                ("freq_per_chan", C.c_uint32), ("polarizations", C.c_uint32),
+                ("row_selection", C.c_int), ("phase_on", C.c_int), ("resolution", C.c_double),
+                ("wmin", C.c_double), ("wmax", C.c_double), ("uu", C.c_void_p),
+                ("vv", C.c_void_p), ("ww", C.c_void_p), ("weight", C.c_void_p),
+                ("vis_real", C.c_void_p), ("vis_img", C.c_void_p), ("image_real", C.c_void_p),
+                ("image_imag", C.c_void_p)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("max_chunk", C.c_uint32), ("grid_blocks_per_sm", C.c_int),
+                ("planes_in_flight", C.c_int)]
+
+
 _lib = None
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -107,6 +123,15 @@ def lib():
     L.rick_plan_get_stats.argtypes = [_vp, C.POINTER(PlanStats)]
     L.rick_plan_set_timing.argtypes = [_vp, C.c_int]
     L.rick_plan_stage_ms.argtypes = [_vp, C.POINTER(C.c_float), C.c_int]
+    L.rick_batch_footprint.argtypes = [C.POINTER(JobDesc), C.c_int, C.c_int,
+                                       C.POINTER(C.c_uint64)]
+    L.rick_batch_create.argtypes = [C.POINTER(_vp), C.POINTER(JobDesc), C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(BatchTuning)]
+    L.rick_batch_run.argtypes = [_vp, _vp]
+    L.rick_batch_get_tuning.argtypes = [_vp, C.POINTER(BatchTuning)]
+    L.rick_batch_get_stats.argtypes = [_vp, C.POINTER(PlanStats)]
+    L.rick_batch_destroy.argtypes = [_vp]
+    L.rick_batch_kernels_per_run.argtypes = [_vp, C.POINTER(C.c_uint32)]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
     L.rick_launch_count.argtypes = []
     L.rick_launch_count.restype = C.c_ulonglong
@@ -114,7 +139,9 @@ def lib():
                "rick_plan_fft", "rick_plan_phase", "rick_plan_image", "rick_plan_image_host",
                "rick_plan_export_cube", "rick_plan_import_cube", "rick_plan_get_stats",
                "rick_kernel_names", "rick_fft_planes", "rick_plan_set_timing",
-               "rick_plan_stage_ms"]:
+               "rick_plan_stage_ms", "rick_batch_footprint", "rick_batch_create",
+               "rick_batch_run", "rick_batch_get_tuning", "rick_batch_get_stats",
+               "rick_batch_destroy", "rick_batch_kernels_per_run"]:
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L
@@ -316,6 +343,102 @@ class Plan:
         s = PlanStats()
         check(lib().rick_plan_get_stats(self._h, C.byref(s)), "rick_plan_get_stats")
         return {k: int(getattr(s, k)) for k, _ in PlanStats._fields_}
+
+
+# ---- batched imaging --------------------------------------------------------
+
+@dataclass
+class Job:
+    """One imaging job of a batch: geometry, device rows (uu, vv, ww, weights,
+    vis_re, vis_im as torch CUDA tensors or addresses) and device image planes."""
+    geom: Geometry
+    nrows: int
+    freq_per_chan: int
+    polarizations: int
+    rows: tuple
+    resolution: float
+    wmin: float
+    wmax: float
+    image_re: object
+    image_im: object
+    selection: int = ROWS_ALL
+
+    def desc(self) -> JobDesc:
+        g = self.geom
+        r = [_ptr(x) for x in self.rows]
+        return JobDesc(g.grid_size_x, g.grid_size_y, g.num_w_planes, g.w_support,
+                       KERNELS[g.kernel], self.nrows,
+                       self.freq_per_chan, self.polarizations, self.selection,
+                       int(bool(g.phase_on)), self.resolution, self.wmin, self.wmax, *r,
+                       _ptr(self.image_re), _ptr(self.image_im))
+
+
+def _descs(jobs):
+    arr = (JobDesc * len(jobs))()
+    for i, j in enumerate(jobs):
+        arr[i] = j.desc()
+    return arr
+
+
+class Batch:
+    """Many imaging jobs run as one launch per stage, captured in a CUDA graph
+    (include/rick_b200.h, section 4).  ``tuning=None`` autotunes."""
+
+    def __init__(self, jobs, precision="mixed", device=0, tuning: Optional[dict] = None):
+        self._keep = list(jobs)  # the descriptors hold raw device addresses
+        descs = _descs(self._keep)
+        t = None
+        if tuning is not None:
+            t = BatchTuning(tuning["max_chunk"], tuning["grid_blocks_per_sm"],
+                            tuning["planes_in_flight"])
+        h = _vp()
+        check(lib().rick_batch_create(C.byref(h), descs, len(descs), PRECISIONS[precision],
+                                      device, C.byref(t) if t is not None else None),
+              "rick_batch_create")
+        self._h = h
+
+    @staticmethod
+    def footprint(jobs, precision="mixed") -> int:
+        descs = _descs(list(jobs))
+        b = C.c_uint64()
+        check(lib().rick_batch_footprint(descs, len(descs), PRECISIONS[precision], C.byref(b)),
+              "rick_batch_footprint")
+        return int(b.value)
+
+    def run(self, stream=None):
+        check(lib().rick_batch_run(self._h, _stream(stream)), "rick_batch_run")
+
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        check(lib().rick_batch_get_tuning(self._h, C.byref(t)), "rick_batch_get_tuning")
+        return {k: int(getattr(t, k)) for k, _ in BatchTuning._fields_}
+
+    def kernels_per_run(self) -> int:
+        k = C.c_uint32()
+        check(lib().rick_batch_kernels_per_run(self._h, C.byref(k)), "rick_batch_kernels_per_run")
+        return int(k.value)
+
+    def stats(self) -> dict:
+        s = PlanStats()
+        check(lib().rick_batch_get_stats(self._h, C.byref(s)), "rick_batch_get_stats")
+        return {k: int(getattr(s, k)) for k, _ in PlanStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rick_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def resolution_of(meta: dict) -> float:

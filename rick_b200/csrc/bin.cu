@@ -78,34 +78,72 @@ __device__ __forceinline__ void footprint_bins(const RowPos &p, const Geometry &
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
-// Pass 1: histogram of records per bin.  One row per lane; lanes of a warp that
-// hit the same bin combine their increments (the uv centre is dense).
+__device__ __forceinline__ void offset_bins(uint32_t bins[4], uint32_t bin_base) {
+#pragma unroll
+  for (int s = 0; s < 4; s++) bins[s] = bins[s] == kNoBin ? kNoBin : bins[s] + bin_base;
+}
+
+// Pass 1 over rows base..base+31 (one per lane): histogram of records per bin.
+// Lanes of a warp that hit the same bin combine their increments (the uv
+// centre is dense).  Returns 1 on a lane whose row was dropped.
+__device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
+                                               const double *__restrict__ vv,
+                                               const double *__restrict__ ww, uint64_t nrows,
+                                               const Geometry &g, uint64_t base,
+                                               uint32_t bin_base, uint32_t *__restrict__ bin_count) {
+  const unsigned lane = lane_id();
+  const uint64_t i = base + lane;
+  RowPos p;
+  p.keep = false;
+  uint32_t dropped = 0;
+  if (i < nrows) {
+    p = row_position(uu[i], vv[i], ww[i], g);
+    dropped = p.keep ? 0u : 1u;
+  }
+  uint32_t bins[4];
+  footprint_bins(p, g, bins);
+  offset_bins(bins, bin_base);
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const unsigned peers = __match_any_sync(kFull, bins[s]);
+    const unsigned leader = __ffs(peers) - 1;
+    if (bins[s] != kNoBin && lane == leader) atomicAdd(&bin_count[bins[s]], __popc(peers));
+  }
+  return dropped;
+}
+
+__device__ __forceinline__ void add_dropped(uint32_t dropped, uint64_t *counters) {
+  for (int o = 16; o; o >>= 1) dropped += __shfl_xor_sync(kFull, dropped, o);
+  if (lane_id() == 0 && dropped) atomicAdd((unsigned long long *)&counters[kCntDropped], dropped);
+}
+
 __global__ void k_bin_count(const double *__restrict__ uu, const double *__restrict__ vv,
                             const double *__restrict__ ww, uint64_t nrows, Geometry g,
                             uint32_t *__restrict__ bin_count, uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
-  const unsigned lane = lane_id();
   uint32_t dropped = 0;
-  for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32) {
-    const uint64_t i = base + lane;
-    RowPos p;
-    p.keep = false;
-    if (i < nrows) {
-      p = row_position(uu[i], vv[i], ww[i], g);
-      dropped += p.keep ? 0u : 1u;
-    }
-    uint32_t bins[4];
-    footprint_bins(p, g, bins);
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const unsigned peers = __match_any_sync(kFull, bins[s]);
-      const unsigned leader = __ffs(peers) - 1;
-      if (bins[s] != kNoBin && lane == leader) atomicAdd(&bin_count[bins[s]], __popc(peers));
-    }
+  for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32)
+    dropped += count_rows(uu, vv, ww, nrows, g, base, 0, bin_count);
+  add_dropped(dropped, counters);
+}
+
+// The same over every job of a batch: one warp per 32-row unit of one job.
+__global__ void k_bin_count_batch(const BatchJob *__restrict__ jobs, int njobs,
+                                  const uint64_t *__restrict__ row_units, uint64_t total_units,
+                                  uint32_t *__restrict__ bin_count,
+                                  uint64_t *__restrict__ counters) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  uint32_t dropped = 0;
+  for (uint64_t u = warp; u < total_units; u += nwarps) {
+    const int j = batch_job_of(row_units, njobs, u);
+    const BatchJob &J = jobs[j];
+    const Geometry g = J.g;
+    dropped += count_rows(J.uu, J.vv, J.ww, J.nrows, g, (u - row_units[j]) * 32, J.bin_base,
+                          bin_count);
   }
-  for (int o = 16; o; o >>= 1) dropped += __shfl_xor_sync(kFull, dropped, o);
-  if (lane == 0 && dropped) atomicAdd((unsigned long long *)&counters[kCntDropped], dropped);
+  add_dropped(dropped, counters);
 }
 
 // Work items of the gridder: a bin with c records is split into ceil(c/max_chunk)
@@ -119,10 +157,118 @@ __global__ void k_item_count(const uint32_t *__restrict__ bin_off, uint64_t nbin
   }
 }
 
-// Pass 2: row sums and record scatter.  A warp owns 32 consecutive rows.  Each
-// group of G lanes reduces one row's samples with 16-byte loads (V4) or scalar
-// loads; after G rounds every lane holds the sum of "its" row, and the records
-// are scattered one row per lane with warp-combined cursor increments.
+// Pass 2 over rows base..base+31: row sums and record scatter.  Each group of
+// G lanes reduces one row's samples with 16-byte loads (V4) or scalar loads;
+// after G rounds every lane holds the sum of "its" row, and the records are
+// scattered one row per lane with warp-combined cursor increments.
+template <int G, bool V4>
+__device__ __forceinline__ void scatter_rows(
+    const double *__restrict__ uu, const double *__restrict__ vv, const double *__restrict__ ww,
+    const float *__restrict__ weight, const float *__restrict__ vis_re,
+    const float *__restrict__ vis_im, uint64_t nrows, uint32_t nchan, uint32_t npol,
+    const Geometry &g, uint64_t base, uint32_t bin_base, const uint32_t *__restrict__ bin_off,
+    uint32_t *__restrict__ bin_cursor, RecF64 *__restrict__ rec, uint32_t &gridded,
+    uint32_t &nrec) {
+  constexpr int R = 32 / G;  // rows per round
+  const unsigned lane = lane_id();
+  const unsigned sub = lane % G, grp = lane / G;
+  const uint64_t nv = (uint64_t)nchan * npol;
+  double my_re = 0.0, my_im = 0.0;
+#pragma unroll 1
+  for (int round = 0; round < G; round++) {
+    const uint64_t i = base + (uint64_t)round * R + grp;
+    double sre = 0.0, sim = 0.0;
+    if (i < nrows) {
+      const float *wrow = weight + i * npol;
+      if (V4) {
+        // npol divides 4, so component c of every float4 is polarisation c % npol
+        float wc[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) wc[c] = __ldg(wrow + (c % npol));
+        const float4 *r4 = reinterpret_cast<const float4 *>(vis_re + i * nv);
+        const float4 *i4 = reinterpret_cast<const float4 *>(vis_im + i * nv);
+        const uint64_t nq = nv / 4;
+#pragma unroll 2
+        for (uint64_t q = sub; q < nq; q += G) {
+          const float4 a = __ldcs(r4 + q);
+          const float4 b = __ldcs(i4 + q);
+          const float ar[4] = {a.x, a.y, a.z, a.w}, bi[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            if (!isnan(ar[c])) {
+              sre += (double)__fmul_rn(wc[c], ar[c]);
+              sim += (double)__fmul_rn(wc[c], bi[c]);
+            }
+          }
+        }
+      } else {
+        for (uint64_t q = sub; q < nv; q += G) {
+          const float a = __ldcs(vis_re + i * nv + q);
+          if (!isnan(a)) {
+            const float wq = __ldg(wrow + (q % npol));
+            sre += (double)__fmul_rn(wq, a);
+            sim += (double)__fmul_rn(wq, __ldcs(vis_im + i * nv + q));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+      sre += __shfl_xor_sync(kFull, sre, o);
+      sim += __shfl_xor_sync(kFull, sim, o);
+    }
+    // lane (round*R + grp') receives the sum of group grp' (its sub-lane 0)
+    const int src = (int)(lane - round * R) * G;
+    const double t_re = __shfl_sync(kFull, sre, src & 31);
+    const double t_im = __shfl_sync(kFull, sim, src & 31);
+    if (lane / R == (unsigned)round) {
+      my_re = t_re;
+      my_im = t_im;
+    }
+  }
+
+  const uint64_t i = base + lane;
+  RowPos p;
+  p.keep = false;
+  if (i < nrows) p = row_position(uu[i], vv[i], ww[i], g);
+  uint32_t bins[4];
+  footprint_bins(p, g, bins);
+  offset_bins(bins, bin_base);
+  gridded += p.keep ? 1u : 0u;
+  RecF64 r;
+  r.sre = my_re;
+  r.sim = my_im;
+  r.fu = p.pu - (double)p.gu;  // exact (Sterbenz)
+  r.fv = p.pv - (double)p.gv;
+  r.gu = p.gu;
+  r.gv = p.gv;
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const unsigned peers = __match_any_sync(kFull, bins[s]);
+    const unsigned leader = __ffs(peers) - 1;
+    uint32_t slot = 0;
+    if (bins[s] != kNoBin && lane == leader) slot = atomicAdd(&bin_cursor[bins[s]], __popc(peers));
+    slot = __shfl_sync(kFull, slot, leader);
+    if (bins[s] != kNoBin) {
+      slot += __popc(peers & ((1u << lane) - 1u));
+      rec[(uint64_t)bin_off[bins[s]] + slot] = r;
+      nrec++;
+    }
+  }
+}
+
+__device__ __forceinline__ void add_scatter_counts(uint32_t gridded, uint32_t nrec,
+                                                   uint64_t *counters) {
+  for (int o = 16; o; o >>= 1) {
+    gridded += __shfl_xor_sync(kFull, gridded, o);
+    nrec += __shfl_xor_sync(kFull, nrec, o);
+  }
+  if (lane_id() == 0) {
+    if (gridded) atomicAdd((unsigned long long *)&counters[kCntGridded], gridded);
+    if (nrec) atomicAdd((unsigned long long *)&counters[kCntRecords], nrec);
+  }
+}
+
 template <int G, bool V4>
 __global__ void __launch_bounds__(256)
     k_bin_scatter(const double *__restrict__ uu, const double *__restrict__ vv,
@@ -131,105 +277,33 @@ __global__ void __launch_bounds__(256)
                   uint64_t nrows, uint32_t nchan, uint32_t npol, Geometry g,
                   const uint32_t *__restrict__ bin_off, uint32_t *__restrict__ bin_cursor,
                   RecF64 *__restrict__ rec, uint64_t *__restrict__ counters) {
-  constexpr int R = 32 / G;  // rows per round
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
-  const unsigned lane = lane_id();
-  const unsigned sub = lane % G, grp = lane / G;
-  const uint64_t nv = (uint64_t)nchan * npol;
   uint32_t gridded = 0, nrec = 0;
+  for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32)
+    scatter_rows<G, V4>(uu, vv, ww, weight, vis_re, vis_im, nrows, nchan, npol, g, base, 0,
+                        bin_off, bin_cursor, rec, gridded, nrec);
+  add_scatter_counts(gridded, nrec, counters);
+}
 
-  for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32) {
-    double my_re = 0.0, my_im = 0.0;
-#pragma unroll 1
-    for (int round = 0; round < G; round++) {
-      const uint64_t i = base + (uint64_t)round * R + grp;
-      double sre = 0.0, sim = 0.0;
-      if (i < nrows) {
-        const float *wrow = weight + i * npol;
-        if (V4) {
-          // npol divides 4, so component c of every float4 is polarisation c % npol
-          float wc[4];
-#pragma unroll
-          for (int c = 0; c < 4; c++) wc[c] = __ldg(wrow + (c % npol));
-          const float4 *r4 = reinterpret_cast<const float4 *>(vis_re + i * nv);
-          const float4 *i4 = reinterpret_cast<const float4 *>(vis_im + i * nv);
-          const uint64_t nq = nv / 4;
-#pragma unroll 2
-          for (uint64_t q = sub; q < nq; q += G) {
-            const float4 a = __ldcs(r4 + q);
-            const float4 b = __ldcs(i4 + q);
-            const float ar[4] = {a.x, a.y, a.z, a.w}, bi[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-              if (!isnan(ar[c])) {
-                sre += (double)__fmul_rn(wc[c], ar[c]);
-                sim += (double)__fmul_rn(wc[c], bi[c]);
-              }
-            }
-          }
-        } else {
-          for (uint64_t q = sub; q < nv; q += G) {
-            const float a = __ldcs(vis_re + i * nv + q);
-            if (!isnan(a)) {
-              const float wq = __ldg(wrow + (q % npol));
-              sre += (double)__fmul_rn(wq, a);
-              sim += (double)__fmul_rn(wq, __ldcs(vis_im + i * nv + q));
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int o = G / 2; o; o >>= 1) {
-        sre += __shfl_xor_sync(kFull, sre, o);
-        sim += __shfl_xor_sync(kFull, sim, o);
-      }
-      // lane (round*R + grp') receives the sum of group grp' (its sub-lane 0)
-      const int src = (int)(lane - round * R) * G;
-      const double t_re = __shfl_sync(kFull, sre, src & 31);
-      const double t_im = __shfl_sync(kFull, sim, src & 31);
-      if (lane / R == (unsigned)round) {
-        my_re = t_re;
-        my_im = t_im;
-      }
-    }
-
-    const uint64_t i = base + lane;
-    RowPos p;
-    p.keep = false;
-    if (i < nrows) p = row_position(uu[i], vv[i], ww[i], g);
-    uint32_t bins[4];
-    footprint_bins(p, g, bins);
-    gridded += p.keep ? 1u : 0u;
-    RecF64 r;
-    r.sre = my_re;
-    r.sim = my_im;
-    r.fu = p.pu - (double)p.gu;  // exact (Sterbenz)
-    r.fv = p.pv - (double)p.gv;
-    r.gu = p.gu;
-    r.gv = p.gv;
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const unsigned peers = __match_any_sync(kFull, bins[s]);
-      const unsigned leader = __ffs(peers) - 1;
-      uint32_t slot = 0;
-      if (bins[s] != kNoBin && lane == leader) slot = atomicAdd(&bin_cursor[bins[s]], __popc(peers));
-      slot = __shfl_sync(kFull, slot, leader);
-      if (bins[s] != kNoBin) {
-        slot += __popc(peers & ((1u << lane) - 1u));
-        rec[(uint64_t)bin_off[bins[s]] + slot] = r;
-        nrec++;
-      }
-    }
+template <int G, bool V4>
+__global__ void __launch_bounds__(256)
+    k_bin_scatter_batch(const BatchJob *__restrict__ jobs, int njobs,
+                        const uint64_t *__restrict__ row_units, uint64_t total_units,
+                        const uint32_t *__restrict__ bin_off, uint32_t *__restrict__ bin_cursor,
+                        RecF64 *__restrict__ rec, uint64_t *__restrict__ counters) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  uint32_t gridded = 0, nrec = 0;
+  for (uint64_t u = warp; u < total_units; u += nwarps) {
+    const int j = batch_job_of(row_units, njobs, u);
+    const BatchJob &J = jobs[j];
+    const Geometry g = J.g;
+    scatter_rows<G, V4>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan,
+                        J.npol, g, (u - row_units[j]) * 32, J.bin_base, bin_off, bin_cursor, rec,
+                        gridded, nrec);
   }
-  for (int o = 16; o; o >>= 1) {
-    gridded += __shfl_xor_sync(kFull, gridded, o);
-    nrec += __shfl_xor_sync(kFull, nrec, o);
-  }
-  if (lane == 0) {
-    if (gridded) atomicAdd((unsigned long long *)&counters[kCntGridded], gridded);
-    if (nrec) atomicAdd((unsigned long long *)&counters[kCntRecords], nrec);
-  }
+  add_scatter_counts(gridded, nrec, counters);
 }
 
 template <int G, bool V4>
@@ -244,6 +318,8 @@ void launch_scatter(int blocks, cudaStream_t st, const double *uu, const double 
 }
 
 }  // namespace
+
+int lanes_per_row(uint64_t per_row);
 
 int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
              const double *vv, const double *ww, const float *weight, const float *vis_re,
@@ -280,8 +356,7 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
   const bool v4 = aligned && nv % 4 == 0 && (npol == 1 || npol == 2 || npol == 4);
   const uint64_t per_row = v4 ? nv / 4 : nv;
   // lanes per row: enough to cover a row's 16-byte chunks in one or two sweeps
-  int G = 1;
-  while (G < 32 && (uint64_t)G * 2 <= per_row) G *= 2;
+  const int G = lanes_per_row(per_row);
   const int blocks = (int)std::min<uint64_t>((warps_needed + 7) / 8, (uint64_t)sms * 8);
 #define RICK_SCATTER(GG)                                                                    \
   case GG:                                                                                  \
@@ -301,6 +376,60 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
     RICK_SCATTER(32)
   }
 #undef RICK_SCATTER
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
+// Lanes that share one row's samples: enough to cover the row's loads in one
+// or two sweeps; rows of at most 8 loads are read by one lane each (a row
+// spread over lanes would leave each lane one load and the warp waiting).
+int lanes_per_row(uint64_t per_row) {
+  if (per_row <= 8) return 1;
+  int G = 1;
+  while (G < 32 && (uint64_t)G * 2 <= per_row) G *= 2;
+  return G;
+}
+
+int bin_rows_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cudaStream_t st) {
+  const uint64_t nbins = b.total_bins;
+  RICK_CUDA(cudaMemsetAsync(s.bin_count, 0, (nbins + 1) * sizeof(uint32_t), st));
+  RICK_CUDA(cudaMemsetAsync(s.bin_cursor, 0, std::max<uint64_t>(nbins, 1) * sizeof(uint32_t), st));
+  const int sms = num_sms();
+  const uint64_t units = b.total_row_units;
+  const int blocks_cnt = (int)std::max<uint64_t>(1, std::min<uint64_t>((units + 7) / 8, (uint64_t)sms * 16));
+  RICK_LAUNCHED();
+  k_bin_count_batch<<<blocks_cnt, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units, units,
+                                                s.bin_count, s.counters);
+  RICK_CUDA(cudaGetLastError());
+  RICK_TRY(exclusive_scan_u32(s.bin_count, s.bin_count, nbins + 1, s.scan_tmp, st));
+  const int blocks_items = (int)std::min<uint64_t>((nbins + 256) / 256, (uint64_t)sms * 32);
+  RICK_LAUNCHED();
+  k_item_count<<<blocks_items, 256, 0, st>>>(s.bin_count, nbins, max_chunk, s.item_off);
+  RICK_CUDA(cudaGetLastError());
+  RICK_TRY(exclusive_scan_u32(s.item_off, s.item_off, nbins + 1, s.scan_tmp, st));
+  const int G = lanes_per_row(b.v4 ? (uint64_t)b.max_nv / 4 : (uint64_t)b.max_nv);
+  const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((units + 7) / 8, (uint64_t)sms * 8));
+#define RICK_SCATTER_B(GG)                                                                   \
+  case GG:                                                                                   \
+    RICK_LAUNCHED();                                                                         \
+    if (b.v4)                                                                                \
+      k_bin_scatter_batch<GG, true><<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units,   \
+                                                            units, s.bin_count, s.bin_cursor, \
+                                                            s.records, s.counters);           \
+    else                                                                                     \
+      k_bin_scatter_batch<GG, false><<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units,  \
+                                                             units, s.bin_count, s.bin_cursor, \
+                                                             s.records, s.counters);          \
+    break;
+  switch (G) {
+    RICK_SCATTER_B(1)
+    RICK_SCATTER_B(2)
+    RICK_SCATTER_B(4)
+    RICK_SCATTER_B(8)
+    RICK_SCATTER_B(16)
+    RICK_SCATTER_B(32)
+  }
+#undef RICK_SCATTER_B
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }

@@ -31,11 +31,6 @@ template <typename T> struct V2;
 template <> struct V2<double> { using t = double2; };
 template <> struct V2<float> { using t = float2; };
 
-int ilog2(int n) {
-  int l = 0;
-  while ((1 << l) < n) l++;
-  return l;
-}
 
 template <typename T> struct Cx {
   T re, im;
@@ -400,59 +395,101 @@ template <int LOGN> constexpr int group_threads() { return (1 << LOGN) / kVpt; }
 template <int LOGN> constexpr int block_threads() {
   return group_threads<LOGN>() > 256 ? group_threads<LOGN>() : 256;
 }
+// Blocks of 256 threads (lengths up to 2048) are bounded to 128 registers so
+// that two share an SM.
+template <int LOGN> constexpr int min_blocks() { return block_threads<LOGN>() <= 256 ? 2 : 1; }
 
 // Row pass: inverse FFT along x of the listed touched rows, from the gridded
 // cube into the column-blocked buffer.  Tiles that received no record (bit
 // clear in the band's tile bitmap) were never written and read as zeros.  The
 // last FFT pass leaves each thread's outputs in registers, stored as whole
-// 128-byte lines.
+// 128-byte lines.  One call transforms one row per row group (blockDim / G rows
+// per block); every thread of the block takes part.
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(block_threads<LOGN>())
+__device__ __forceinline__ void fft_row_unit(typename V2<T>::t *s, bool active, uint32_t w,
+                                             uint32_t k, const typename V2<T>::t *__restrict__ cube,
+                                             typename V2<T>::t *__restrict__ out, int nx, int ny,
+                                             int nty, int tmw,
+                                             const uint32_t *__restrict__ tilemask,
+                                             const typename V2<T>::t *__restrict__ tw) {
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  using V = typename V2<T>::t;
+  const int grp = threadIdx.x / G, t = threadIdx.x % G;
+  V *srow = s + grp * LEN;
+  if (!active) w = k = 0;
+  const uint32_t *tm = tilemask + ((uint64_t)w * nty + (k >> 5)) * tmw;
+  const uint64_t rowbase = ((uint64_t)w * ny + k) * nx;
+#pragma unroll
+  for (int q = 0; q < kVpt; q++) {
+    const int x = t + q * G;
+    V v;
+    v.x = 0;
+    v.y = 0;
+    if (active && ((tm[x >> 10] >> ((x >> 5) & 31)) & 1u)) v = cube[rowbase + x];
+    srow[pad(x)] = v;
+  }
+  __syncthreads();
+  Cx<T> res[kVpt];
+  fft_to_regs<T, LOGN>(srow, t, tw, res);
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      V v;
+      v.x = res[q].re;
+      v.y = res[q].im;
+      out[blocked_index<T>(w, k, t + q * G, nx, ny)] = v;
+    }
+  }
+  __syncthreads();
+}
+
+// One job's row pass (the plan): the job's arrays as kernel parameters.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
     k_fft_rows(const typename V2<T>::t *__restrict__ cube, typename V2<T>::t *__restrict__ out,
                int nx, int ny, int nty, int tmw, const uint32_t *__restrict__ tilemask,
                const uint32_t *__restrict__ rowlist, const uint32_t *__restrict__ counts,
                const typename V2<T>::t *__restrict__ tw) {
-  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
-  using V = typename V2<T>::t;
+  constexpr int G = (1 << LOGN) / kVpt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V *s = reinterpret_cast<V *>(smem_raw);
+  auto *s = reinterpret_cast<typename V2<T>::t *>(smem_raw);
   const int rpc = blockDim.x / G;  // rows per CTA
-  const int grp = threadIdx.x / G, t = threadIdx.x % G;
-  V *srow = s + grp * LEN;
+  const int grp = threadIdx.x / G;
   const uint32_t nrows = counts[0];
   for (uint32_t base = blockIdx.x * rpc; base < nrows; base += gridDim.x * rpc) {
     const uint32_t li = base + grp;
     const bool active = li < nrows;
-    uint32_t w = 0, k = 0;
-    if (active) {
-      const uint32_t rid = rowlist[li];
-      w = rid / (uint32_t)ny;
-      k = rid % (uint32_t)ny;
-    }
-    const uint32_t *tm = tilemask + ((uint64_t)w * nty + (k >> 5)) * tmw;
-    const uint64_t rowbase = ((uint64_t)w * ny + k) * nx;
-#pragma unroll
-    for (int q = 0; q < kVpt; q++) {
-      const int x = t + q * G;
-      V v;
-      v.x = 0;
-      v.y = 0;
-      if (active && ((tm[x >> 10] >> ((x >> 5) & 31)) & 1u)) v = cube[rowbase + x];
-      srow[pad(x)] = v;
-    }
-    __syncthreads();
-    Cx<T> res[kVpt];
-    fft_to_regs<T, LOGN>(srow, t, tw, res);
-    if (active) {
-#pragma unroll
-      for (int q = 0; q < kVpt; q++) {
-        V v;
-        v.x = res[q].re;
-        v.y = res[q].im;
-        out[blocked_index<T>(w, k, t + q * G, nx, ny)] = v;
-      }
-    }
-    __syncthreads();
+    const uint32_t rid = active ? rowlist[li] : 0;
+    fft_row_unit<T, LOGN>(s, active, rid / (uint32_t)ny, rid % (uint32_t)ny, cube, out, nx, ny,
+                          nty, tmw, tilemask, tw);
+  }
+}
+
+// Row pass over the jobs lo..hi-1 of a batch (all of FFT length 2^LOGN along x): the
+// row-pass units of job j (groups of rows_per_block touched rows) are
+// fft_units[j] .. fft_units[j+1]-1.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+    k_fft_rows_multi(const BatchJob *__restrict__ jobs, int lo, int hi,
+               const uint32_t *__restrict__ fft_units, const uint32_t *__restrict__ tilemask,
+               const uint32_t *__restrict__ rowlist, const uint32_t *__restrict__ counts) {
+  constexpr int G = (1 << LOGN) / kVpt;
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto *s = reinterpret_cast<V *>(smem_raw);
+  const int rpc = blockDim.x / G;  // rows per CTA
+  const int grp = threadIdx.x / G;
+  const uint32_t u1 = fft_units[hi];
+  for (uint32_t u = fft_units[lo] + blockIdx.x; u < u1; u += gridDim.x) {
+    const int j = lo + batch_job_of(fft_units + lo, hi - lo, u);
+    const BatchJob &J = jobs[j];
+    const uint32_t li = (u - fft_units[j]) * rpc + grp;
+    const bool active = li < counts[J.counts_base];
+    const uint32_t rid = active ? rowlist[J.list_base + li] : 0;
+    const uint32_t ny = (uint32_t)J.g.ny;
+    fft_row_unit<T, LOGN>(s, active, rid / ny, rid % ny, (const V *)J.cube, (V *)J.blocked,
+                          J.g.nx, J.g.ny, J.g.nty, (J.g.ntx + 31) / 32, tilemask + J.tile_base,
+                          (const V *)J.tw_x);
   }
 }
 
@@ -461,10 +498,12 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
 // next plane's column is copied into a second shared buffer (cp.async,
 // untouched rows zero-filled) while the current one is transformed; the last
 // FFT pass leaves the column's values in the registers of the threads that
-// accumulate those pixels.
+// accumulate those pixels.  PP planes share one pass through the FFT's
+// barriers.
 //
 // Phase (phase_correction.cu:51-80): every kAnchor planes (and at the first
-// plane; at every plane without RECUR, when the step table does not fit) the factor exp(i*(2 pi wterm)*(root-1)) is evaluated with sincos of the
+// plane; at every plane without RECUR, when the step table does not fit) the
+// factor exp(i*(2 pi wterm)*(root-1)) is evaluated with sincos of the
 // reference's FP64 argument and scaled by dwnorm*root; between anchors it
 // advances by the per-pixel step exp(i*(2 pi dw)*(root-1)) (shared memory).
 // Over 8 planes the advanced factor differs from a long-double evaluation by
@@ -472,27 +511,47 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
 // less than the rounding of the reference's own argument (~3e-13).
 constexpr int kAnchor = 8;
 
+// The per-job inputs of the column pass.
+template <typename T> struct ColJob {
+  const typename V2<T>::t *cube;  // column-blocked row transforms
+  int nx, ny, nw, nty;
+  const uint32_t *rowmask;        // [nw * nty]
+  const uint32_t *counts;         // [1 + nw]
+  const typename V2<T>::t *tw;    // twiddles of the y axis
+  const double *ltab, *mtab;
+  double wmin, dw, dwnorm, norm;
+  int phase_on;
+  double *img_re, *img_im;
+};
+
+// Shared memory of one block of the column pass: NB column buffers per row
+// group, the per-pixel phase steps (RECUR) and the row masks of 2*PP planes.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
-__global__ void __launch_bounds__(block_threads<LOGN>())
-    k_fft_cols_image(const typename V2<T>::t *__restrict__ cube, int nx, int ny, int nw, int nty,
-                     const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts,
-                     const typename V2<T>::t *__restrict__ tw, const double *__restrict__ ltab,
-                     const double *__restrict__ mtab, double wmin, double dw, double dwnorm,
-                     double norm, int phase_on, double *__restrict__ img_re,
-                     double *__restrict__ img_im) {
+__host__ __device__ constexpr size_t cols_smem_bytes(int rpc) {
+  return (size_t)rpc * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(typename V2<T>::t) *
+             (DB ? 2 : 1) * PP +
+         (RECUR ? (size_t)rpc * (1 << LOGN) * 16 : 0) + 2 * PP * (size_t)((1 << LOGN) / 32) * 4;
+}
+
+// Columns base..base+rpc-1 (one per row group) of one job.
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
+__device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base,
+                                             const ColJob<T> &J) {
   constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
   constexpr int NB = (DB ? 2 : 1) * PP;  // column buffers per row group
   using V = typename V2<T>::t;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V *s = reinterpret_cast<V *>(smem_raw);
   const int rpc = blockDim.x / G;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
+  const int nx = J.nx, ny = J.ny, nw = J.nw, nty = J.nty;
+  const uint32_t *__restrict__ rowmask = J.rowmask;
+  const uint32_t *__restrict__ counts = J.counts;
+  const double *__restrict__ mtab = J.mtab;
   V *sbase = s + grp * NB * LEN;  // buffers [set][pp]: set = cur (DB), pp < PP
   double2 *tables = reinterpret_cast<double2 *>(s + rpc * NB * LEN);
   double2 *sstep = tables + grp * N;  // RECUR only
   // row masks of the planes of the next two sets (2 * PP slots)
   uint32_t *smask = reinterpret_cast<uint32_t *>(tables + (RECUR ? rpc * N : 0));
-  const bool phase = phase_on && nw > 1;
+  const bool phase = J.phase_on && nw > 1;
   const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
   auto next_plane = [&](int iw) {
     do { iw++; } while (iw < nw && counts[1 + iw] == 0);  // planes without data add exact zeros
@@ -513,14 +572,16 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
       if (set[pp] < nw) smask[(slot * PP + pp) * nty + word] = rowmask[(uint64_t)set[pp] * nty + word];
     }
   };
-  auto load_set = [&](int bset, const int set[PP], int slot, uint32_t n, bool active) {
+  const uint32_t n = base + grp;
+  const bool active = n < (uint32_t)nx;
+  auto load_set = [&](int bset, const int set[PP], int slot) {
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
       if (set[pp] >= nw) continue;
       V *dst = sbase + (bset * PP + pp) * LEN;
       const uint32_t *mask = smask + (slot * PP + pp) * nty;
       constexpr int CB = col_block<T>();
-      const V *col = cube + blocked_index<T>(set[pp], 0, active ? n : 0, nx, ny);
+      const V *col = J.cube + blocked_index<T>(set[pp], 0, active ? n : 0, nx, ny);
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int k = t + q * G;
@@ -542,141 +603,208 @@ __global__ void __launch_bounds__(block_threads<LOGN>())
     const double mm = mtab[m];
     return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
   };
-  const double dwstep = __dmul_rn(twopi, dw);
-  for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)nx; base += gridDim.x * rpc) {
-    const uint32_t n = base + grp;
-    const bool active = n < (uint32_t)nx;
-    const double l = active ? ltab[n] : 0.0;
-    double acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
+  const double dwstep = __dmul_rn(twopi, J.dw);
+  const double l = active ? J.ltab[n] : 0.0;
+  double acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
 #pragma unroll
-    for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = 0.0;
-    int cur[PP], nxt[PP];
-    next_set(-1, cur);
-    next_set(cur[PP - 1], nxt);
-    stage_masks(0, cur);
-    stage_masks(1, nxt);
-    if (phase && RECUR) {
+  for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = 0.0;
+  int cur[PP], nxt[PP];
+  next_set(-1, cur);
+  next_set(cur[PP - 1], nxt);
+  stage_masks(0, cur);
+  stage_masks(1, nxt);
+  if (phase && RECUR) {
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      const int m = t + q * G;
+      double sn, cs;
+      sincos(__dmul_rn(dwstep, __dsub_rn(root_of(l, m), 1.0)), &sn, &cs);
+      sstep[m] = make_double2(cs, sn);
+    }
+  }
+  __syncthreads();
+  if (DB && cur[0] < nw) {
+    load_set(0, cur, 0);
+    cp_async_commit();
+  }
+  int bset = 0, it = 0;
+  int last_anchor = -kAnchor, prev_iw = -1;
+  while (cur[0] < nw) {
+    int nn[PP];
+    next_set(nxt[PP - 1], nn);  // the set after the next one
+    if (DB) {
+      if (nxt[0] < nw) load_set(bset ^ 1, nxt, (it + 1) & 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      load_set(0, cur, it & 1);
+    }
+    __syncthreads();
+    // this set's mask slot is free now: stage the set after next
+    stage_masks(it & 1, nn);
+    V *bufs[PP];
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) bufs[pp] = sbase + ((DB ? bset : 0) * PP + pp) * LEN;
+    Cx<T> x[PP][kVpt];
+    fft_to_regs_pp<T, LOGN, PP>(bufs, t, J.tw, x);
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) {
+      const int iw = cur[pp];
+      if (iw >= nw) break;
+      const bool anchor = !RECUR || iw - last_anchor >= kAnchor;
+      const int gap = iw - prev_iw;  // planes since the previous factor (empty planes skipped)
+      double cw = 0.0;
+      if (anchor) {
+        last_anchor = iw;
+        cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)iw, J.dw)));  // 2 pi wterm
+      }
+      prev_iw = iw;
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int m = t + q * G;
-        double sn, cs;
-        sincos(__dmul_rn(dwstep, __dsub_rn(root_of(l, m), 1.0)), &sn, &cs);
-        sstep[m] = make_double2(cs, sn);
+        const double p = __dmul_rn(J.norm, (double)x[pp][q].re);
+        const double qq = __dmul_rn(J.norm, (double)x[pp][q].im);
+        if (phase) {
+          if (anchor) {
+            const double root = root_of(l, m);
+            double sn, cs;
+            sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+            const double amp = J.dwnorm * root;
+            ph_re[q] = cs * amp;
+            ph_im[q] = sn * amp;
+          } else {
+            const double2 st = sstep[m];
+            double sr = st.x, si = st.y;
+            for (int g2 = 1; g2 < gap; g2++) {
+              const double tr = sr * st.x - si * st.y;
+              si = sr * st.y + si * st.x;
+              sr = tr;
+            }
+            const double tr = ph_re[q] * sr - ph_im[q] * si;
+            ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
+            ph_re[q] = tr;
+          }
+          acc_re[q] += p * ph_re[q] - qq * ph_im[q];
+          acc_im[q] += p * ph_im[q] + qq * ph_re[q];
+        } else {
+          acc_re[q] += p;
+          acc_im[q] += qq;
+        }
       }
     }
     __syncthreads();
-    if (DB && cur[0] < nw) {
-      load_set(0, cur, 0, n, active);
-      cp_async_commit();
+    if (DB) bset ^= 1;
+#pragma unroll
+    for (int pp = 0; pp < PP; pp++) {
+      cur[pp] = nxt[pp];
+      nxt[pp] = nn[pp];
     }
-    int bset = 0, it = 0;
-    int last_anchor = -kAnchor, prev_iw = -1;
-    while (cur[0] < nw) {
-      int nn[PP];
-      next_set(nxt[PP - 1], nn);  // the set after the next one
-      if (DB) {
-        if (nxt[0] < nw) load_set(bset ^ 1, nxt, (it + 1) & 1, n, active);
-        cp_async_commit();
-        cp_async_wait<1>();
-      } else {
-        load_set(0, cur, it & 1, n, active);
-      }
-      __syncthreads();
-      // this set's mask slot is free now: stage the set after next
-      stage_masks(it & 1, nn);
-      V *bufs[PP];
+    it++;
+  }
+  if (DB) cp_async_wait<0>();
+  if (active) {
 #pragma unroll
-      for (int pp = 0; pp < PP; pp++) bufs[pp] = sbase + ((DB ? bset : 0) * PP + pp) * LEN;
-      Cx<T> x[PP][kVpt];
-      fft_to_regs_pp<T, LOGN, PP>(bufs, t, tw, x);
-#pragma unroll
-      for (int pp = 0; pp < PP; pp++) {
-        const int iw = cur[pp];
-        if (iw >= nw) break;
-        const bool anchor = !RECUR || iw - last_anchor >= kAnchor;
-        const int gap = iw - prev_iw;  // planes since the previous factor (empty planes skipped)
-        double cw = 0.0;
-        if (anchor) {
-          last_anchor = iw;
-          cw = __dmul_rn(twopi, __dadd_rn(wmin, __dmul_rn((double)iw, dw)));  // 2 pi wterm
-        }
-        prev_iw = iw;
-#pragma unroll
-        for (int q = 0; q < kVpt; q++) {
-          const int m = t + q * G;
-          const double p = __dmul_rn(norm, (double)x[pp][q].re);
-          const double qq = __dmul_rn(norm, (double)x[pp][q].im);
-          if (phase) {
-            if (anchor) {
-              const double root = root_of(l, m);
-              double sn, cs;
-              sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
-              const double amp = dwnorm * root;
-              ph_re[q] = cs * amp;
-              ph_im[q] = sn * amp;
-            } else {
-              const double2 st = sstep[m];
-              double sr = st.x, si = st.y;
-              for (int g2 = 1; g2 < gap; g2++) {
-                const double tr = sr * st.x - si * st.y;
-                si = sr * st.y + si * st.x;
-                sr = tr;
-              }
-              const double tr = ph_re[q] * sr - ph_im[q] * si;
-              ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
-              ph_re[q] = tr;
-            }
-            acc_re[q] += p * ph_re[q] - qq * ph_im[q];
-            acc_im[q] += p * ph_im[q] + qq * ph_re[q];
-          } else {
-            acc_re[q] += p;
-            acc_im[q] += qq;
-          }
-        }
-      }
-      __syncthreads();
-      if (DB) bset ^= 1;
-#pragma unroll
-      for (int pp = 0; pp < PP; pp++) {
-        cur[pp] = nxt[pp];
-        nxt[pp] = nn[pp];
-      }
-      it++;
+    for (int q = 0; q < kVpt; q++) {
+      const int m = t + q * G;
+      J.img_re[(uint64_t)m * nx + n] = acc_re[q];
+      J.img_im[(uint64_t)m * nx + n] = acc_im[q];
     }
-    if (DB) cp_async_wait<0>();
-    if (active) {
-#pragma unroll
-      for (int q = 0; q < kVpt; q++) {
-        const int m = t + q * G;
-        img_re[(uint64_t)m * nx + n] = acc_re[q];
-        img_im[(uint64_t)m * nx + n] = acc_im[q];
-      }
-    }
-    __syncthreads();  // sstep / smask are rewritten for the next column
+  }
+  __syncthreads();  // sstep / smask are rewritten for the next column
+}
+
+// One job's column pass (the plan): the job as a kernel parameter.
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
+__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+    k_fft_cols_image(ColJob<T> J) {
+  constexpr int G = (1 << LOGN) / kVpt;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto *s = reinterpret_cast<typename V2<T>::t *>(smem_raw);
+  const int rpc = blockDim.x / G;
+  for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)J.nx; base += gridDim.x * rpc)
+    fft_col_unit<T, LOGN, DB, RECUR, PP>(s, base, J);
+}
+
+// Column pass over the jobs col_jobs[lo..hi-1] of a batch (all of FFT length 2^LOGN
+// along y): the column groups of the k-th listed job are col_units[k] ..
+// col_units[k+1]-1.
+template <typename T, int LOGN, bool DB, bool RECUR, int PP>
+__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+    k_fft_cols_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
+                     int lo, int hi, const uint32_t *__restrict__ col_units,
+                     const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts) {
+  constexpr int G = (1 << LOGN) / kVpt;
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto *s = reinterpret_cast<V *>(smem_raw);
+  const int rpc = blockDim.x / G;
+  const uint32_t u1 = col_units[hi];
+  for (uint32_t u = col_units[lo] + blockIdx.x; u < u1; u += gridDim.x) {
+    const int k = lo + batch_job_of(col_units + lo, hi - lo, u);
+    const BatchJob &B = jobs[col_jobs[k]];
+    ColJob<T> J;
+    J.cube = (const V *)B.blocked;
+    J.nx = B.g.nx;
+    J.ny = B.g.ny;
+    J.nw = B.g.nw;
+    J.nty = B.g.nty;
+    J.rowmask = rowmask + B.mask_base;
+    J.counts = counts + B.counts_base;
+    J.tw = (const V *)B.tw_y;
+    J.ltab = B.ltab;
+    J.mtab = B.mtab;
+    J.wmin = B.wmin;
+    J.dw = B.dw_phase;
+    J.dwnorm = B.dwnorm;
+    J.norm = B.norm;
+    J.phase_on = B.phase_on;
+    J.img_re = B.img_re;
+    J.img_im = B.img_im;
+    fft_col_unit<T, LOGN, DB, RECUR, PP>(s, (u - col_units[k]) * (uint32_t)rpc, J);
   }
 }
 
-// Compacts the row mask into the list of touched (plane, row) ids and per-plane
-// counts: counts[0] = rows, counts[1 + w] = touched rows of plane w.
-__global__ void k_row_list(const uint32_t *__restrict__ rowmask, int nw, int ny, int nty,
-                           uint32_t *__restrict__ rowlist, uint32_t *__restrict__ counts) {
-  const uint64_t nwords = (uint64_t)nw * nty;
+// Compacts the row masks of every job into its list of touched (plane, row)
+// ids and per-plane counts: counts[0] = rows, counts[1 + w] = touched rows of
+// plane w (at the job's counts_base).
+__global__ void k_row_list(const BatchJob *__restrict__ jobs, int njobs,
+                           const uint64_t *__restrict__ mask_base, uint64_t nwords,
+                           const uint32_t *__restrict__ rowmask, uint32_t *__restrict__ rowlist,
+                           uint32_t *__restrict__ counts) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nwords;
        i += gridDim.x * (uint64_t)blockDim.x) {
     uint32_t bits = rowmask[i];
     if (!bits) continue;
-    const uint32_t w = (uint32_t)(i / nty), band = (uint32_t)(i % nty);
+    const int j = batch_job_of(mask_base, njobs, i);
+    const BatchJob &J = jobs[j];
+    const uint64_t li = i - J.mask_base;
+    const uint32_t nty = (uint32_t)J.g.nty, ny = (uint32_t)J.g.ny;
+    const uint32_t w = (uint32_t)(li / nty), band = (uint32_t)(li % nty);
     const uint32_t c = __popc(bits);
-    uint32_t slot = atomicAdd(&counts[0], c);
-    atomicAdd(&counts[1 + w], c);
+    uint32_t slot = atomicAdd(&counts[J.counts_base], c);
+    atomicAdd(&counts[J.counts_base + 1 + w], c);
     while (bits) {
       const int b = __ffs(bits) - 1;
       bits &= bits - 1;
       const uint32_t k = band * 32 + b;
-      if (k < (uint32_t)ny) rowlist[slot] = w * (uint32_t)ny + k;
+      if (k < ny) rowlist[J.list_base + slot] = w * ny + k;
       slot++;
     }
   }
+}
+
+// Row-pass units per job (groups of rows_per_block(logx) touched rows),
+// exclusive prefix over the jobs; one thread (a few hundred jobs at most).
+__global__ void k_fft_units(const BatchJob *__restrict__ jobs, int njobs,
+                            const uint32_t *__restrict__ counts, uint32_t *__restrict__ fft_units) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t acc = 0;
+  for (int j = 0; j < njobs; j++) {
+    fft_units[j] = acc;
+    const uint32_t rpc = (uint32_t)fft_rows_per_block(jobs[j].logx);
+    acc += (counts[jobs[j].counts_base] + rpc - 1) / rpc;
+  }
+  fft_units[njobs] = acc;
 }
 
 template <typename T, int LOGN>
@@ -685,79 +813,126 @@ size_t fft_smem(int rpc) {
   return (size_t)rpc * (N + N / 16) * sizeof(typename V2<T>::t);
 }
 
+// Longest transform of the multi-job (batch) kernels: 4096.
+constexpr int kMultiMaxLog = 12;
+
+template <typename T> ColJob<T> col_job(const BatchJob &B, const FftJobs &f) {
+  using V = typename V2<T>::t;
+  ColJob<T> J;
+  J.cube = (const V *)B.blocked;
+  J.nx = B.g.nx;
+  J.ny = B.g.ny;
+  J.nw = B.g.nw;
+  J.nty = B.g.nty;
+  J.rowmask = f.rowmask + B.mask_base;
+  J.counts = f.counts + B.counts_base;
+  J.tw = (const V *)B.tw_y;
+  J.ltab = B.ltab;
+  J.mtab = B.mtab;
+  J.wmin = B.wmin;
+  J.dw = B.dw_phase;
+  J.dwnorm = B.dwnorm;
+  J.norm = B.norm;
+  J.phase_on = B.phase_on;
+  J.img_re = B.img_re;
+  J.img_im = B.img_im;
+  return J;
+}
+
 template <typename T, int LOGN>
-int launch_rows(FftScratch &f, void *cube, const Geometry &g, cudaStream_t st) {
+int launch_rows(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
-  const size_t sm = fft_smem<T, LOGN>(BT / G);
-  RICK_CUDA(cudaFuncSetAttribute(k_fft_rows<T, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm));
-  int per_sm = 0;
-  RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_rows<T, LOGN>, BT, sm));
-  const int blocks = num_sms() * std::max(per_sm, 1);
-  RICK_LAUNCHED();
-  k_fft_rows<T, LOGN><<<blocks, BT, sm, st>>>(
-      (const typename V2<T>::t *)cube, (typename V2<T>::t *)f.blocked, g.nx, g.ny, g.nty,
-      (g.ntx + 31) / 32, f.tilemask, f.rowlist, f.counts,
-      (const typename V2<T>::t *)(sizeof(T) == 8 ? (void *)f.tw_x64 : (void *)f.tw_x32));
+  const int rpc = BT / G;
+  const size_t sm = fft_smem<T, LOGN>(rpc);
+  using V = typename V2<T>::t;
+  if (f.one) {
+    const BatchJob &B = *f.one;
+    RICK_CUDA(cudaFuncSetAttribute(k_fft_rows<T, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sm));
+    int per_sm = 0;
+    RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_rows<T, LOGN>, BT, sm));
+    RICK_LAUNCHED();
+    k_fft_rows<T, LOGN><<<num_sms() * std::max(per_sm, 1), BT, sm, st>>>(
+        (const V *)B.cube, (V *)B.blocked, B.g.nx, B.g.ny, B.g.nty, (B.g.ntx + 31) / 32,
+        f.tilemask + B.tile_base, f.rowlist + B.list_base, f.counts + B.counts_base,
+        (const V *)B.tw_x);
+  } else {
+    if constexpr (LOGN > kMultiMaxLog) {
+      return set_error(RICK_ERR_INVALID_ARG, "batch FFT length above %d", 1 << kMultiMaxLog);
+    } else {
+      RICK_CUDA(cudaFuncSetAttribute(k_fft_rows_multi<T, LOGN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      int per_sm = 0;
+      RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_rows_multi<T, LOGN>,
+                                                              BT, sm));
+      RICK_LAUNCHED();
+      k_fft_rows_multi<T, LOGN><<<num_sms() * std::max(per_sm, 1), BT, sm, st>>>(
+          f.jobs, c.lo, c.hi, f.fft_units, f.tilemask, f.rowlist, f.counts);
+    }
+  }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
 
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 size_t cols_smem(int rpc) {
-  constexpr int N = 1 << LOGN;
-  return fft_smem<T, LOGN>(rpc) * (DB ? 2 : 1) * PP + (RECUR ? (size_t)rpc * N * 16 : 0) +
-         2 * PP * (size_t)(N / 32) * 4;
+  return cols_smem_bytes<T, LOGN, DB, RECUR, PP>(rpc);
 }
 
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
-int launch_cols_impl(FftScratch &f, const Geometry &g, const double *ltab, const double *mtab,
-                     double wmin, double wmax, double norm, int phase_on, double *img_re,
-                     double *img_im, cudaStream_t st) {
+int launch_cols_impl(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
   const int rpc = BT / G;
   const size_t sm = cols_smem<T, LOGN, DB, RECUR, PP>(rpc);
-  RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_image<T, LOGN, DB, RECUR, PP>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int per_sm = 0;
-  RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, k_fft_cols_image<T, LOGN, DB, RECUR, PP>, BT, sm));
-  const int want = (g.nx + rpc - 1) / rpc;
-  const int blocks = std::min(want, num_sms() * std::max(per_sm, 1));
-  // phase_correction.cu:100-102
-  const double dw = (wmax - wmin) / (double)g.nw;
-  const double dwnorm = dw / (wmax - wmin);
-  RICK_LAUNCHED();
-  k_fft_cols_image<T, LOGN, DB, RECUR, PP><<<blocks, BT, sm, st>>>(
-      (const typename V2<T>::t *)f.blocked, g.nx, g.ny, g.nw, g.nty, f.rowmask, f.counts,
-      (const typename V2<T>::t *)(sizeof(T) == 8 ? (void *)f.tw_y64 : (void *)f.tw_y32), ltab,
-      mtab, wmin, dw, dwnorm, norm, phase_on, img_re, img_im);
+  if (f.one) {
+    RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_image<T, LOGN, DB, RECUR, PP>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_fft_cols_image<T, LOGN, DB, RECUR, PP>, BT, sm));
+    const int blocks = (int)std::min<uint64_t>(std::max<uint32_t>(c.units, 1),
+                                               (uint64_t)num_sms() * std::max(per_sm, 1));
+    RICK_LAUNCHED();
+    k_fft_cols_image<T, LOGN, DB, RECUR, PP><<<blocks, BT, sm, st>>>(col_job<T>(*f.one, f));
+  } else {
+    // batch sizes (<= 4096) always fit double-buffered loads and the phase steps
+    if constexpr (LOGN > kMultiMaxLog || !DB || !RECUR) {
+      return set_error(RICK_ERR_INVALID_ARG, "batch FFT length above %d", 1 << kMultiMaxLog);
+    } else {
+      RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_multi<T, LOGN, DB, RECUR, PP>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, k_fft_cols_multi<T, LOGN, DB, RECUR, PP>, BT, sm));
+      const int blocks = (int)std::min<uint64_t>(std::max<uint32_t>(c.units, 1),
+                                                 (uint64_t)num_sms() * std::max(per_sm, 1));
+      RICK_LAUNCHED();
+      k_fft_cols_multi<T, LOGN, DB, RECUR, PP><<<blocks, BT, sm, st>>>(
+          f.jobs, f.col_jobs, c.lo, c.hi, f.col_units, f.rowmask, f.counts);
+    }
+  }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
 
 template <typename T, int LOGN>
-int launch_cols(FftScratch &f, const void *cube, const Geometry &g, const double *ltab,
-                const double *mtab, double wmin, double wmax, double norm, int phase_on,
-                double *img_re, double *img_im, cudaStream_t st) {
+int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
   constexpr int rpc = BT / G;
-  (void)cube;
   // in order of preference, the first that fits: two planes per iteration
   // (FP32), double-buffered loads, the per-pixel phase steps
   constexpr size_t kMax = 220 * 1024;
-#define RICK_TRY_COLS(DB, RC, PP)                                                              \
-  if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)                                             \
-    return launch_cols_impl<T, LOGN, DB, RC, PP>(f, g, ltab, mtab, wmin, wmax, norm, phase_on, \
-                                                 img_re, img_im, st);
+#define RICK_TRY_COLS(DB, RC, PP)                            \
+  if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)           \
+    return launch_cols_impl<T, LOGN, DB, RC, PP>(f, c, st);
   if constexpr (sizeof(T) == 4) {
-    RICK_TRY_COLS(true, true, 2)
+    if (f.cols_pp >= 2) {
+      RICK_TRY_COLS(true, true, 2)
+    }
   }
   RICK_TRY_COLS(true, true, 1)
   RICK_TRY_COLS(false, true, 1)
 #undef RICK_TRY_COLS
-  return launch_cols_impl<T, LOGN, false, false, 1>(f, g, ltab, mtab, wmin, wmax, norm, phase_on,
-                                                    img_re, img_im, st);
+  return launch_cols_impl<T, LOGN, false, false, 1>(f, c, st);
 }
 
 }  // namespace
@@ -793,63 +968,95 @@ void make_twiddles(int n, double2 *t64, float2 *t32) {
   t32[n - 1] = make_float2(1.0f, 0.0f);
 }
 
-int sparse_row_list(FftScratch &f, const Geometry &g, cudaStream_t st) {
-  RICK_CUDA(cudaMemsetAsync(f.counts, 0, sizeof(uint32_t) * (1 + g.nw), st));
-  const uint64_t nwords = (uint64_t)g.nw * g.nty;
+void fft_classes(const BatchJob *jobs, int njobs, FftJobs &f, uint32_t *col_jobs,
+                 uint32_t *col_units) {
+  f.n_row_cls = 0;
+  for (int j = 0; j < njobs; j++) {
+    if (f.n_row_cls == 0 || f.row_cls[f.n_row_cls - 1].log != jobs[j].logx)
+      f.row_cls[f.n_row_cls++] = FftClass{jobs[j].logx, j, j + 1, 0};
+    else
+      f.row_cls[f.n_row_cls - 1].hi = j + 1;
+  }
+  // column pass: the jobs grouped by logy (stable), units = column groups
+  int n = 0;
+  f.n_col_cls = 0;
+  uint32_t acc = 0;
+  for (int l = 6; l <= 13; l++) {
+    const int lo = n;
+    uint32_t units = 0;
+    for (int j = 0; j < njobs; j++) {
+      if (jobs[j].logy != l) continue;
+      col_jobs[n] = (uint32_t)j;
+      col_units[n] = acc;
+      const uint32_t rpc = (uint32_t)fft_rows_per_block(l);
+      const uint32_t u = ((uint32_t)jobs[j].g.nx + rpc - 1) / rpc;
+      acc += u;
+      units += u;
+      n++;
+    }
+    if (n > lo) f.col_cls[f.n_col_cls++] = FftClass{l, lo, n, units};
+  }
+  col_units[n] = acc;
+}
+
+int sparse_fft_lists(const FftJobs &f, cudaStream_t st) {
+  RICK_CUDA(cudaMemsetAsync(f.counts, 0, sizeof(uint32_t) * f.total_count_words, st));
+  const uint64_t nwords = f.total_mask_words;
   const int blocks = (int)std::min<uint64_t>((nwords + 255) / 256, (uint64_t)num_sms() * 8);
   RICK_LAUNCHED();
-  k_row_list<<<std::max(blocks, 1), 256, 0, st>>>(f.rowmask, g.nw, g.ny, g.nty, f.rowlist,
-                                                  f.counts);
+  k_row_list<<<std::max(blocks, 1), 256, 0, st>>>(f.jobs, f.njobs, f.mask_base, nwords,
+                                                  f.rowmask, f.rowlist, f.counts);
+  RICK_CUDA(cudaGetLastError());
+  RICK_LAUNCHED();
+  k_fft_units<<<1, 32, 0, st>>>(f.jobs, f.njobs, f.counts, f.fft_units);
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
 
 #define RICK_FFT_SIZES(X) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
-int sparse_fft_rows(int precision, FftScratch &f, void *cube, const Geometry &g,
-                    cudaStream_t st) {
-  const int lx = ilog2(g.nx);
-  if (precision == RICK_PREC_FP64) {
-    switch (lx) {
-#define X(L) case L: return launch_rows<double, L>(f, cube, g, st);
-      RICK_FFT_SIZES(X)
+int sparse_fft_rows(const FftJobs &f, int precision, cudaStream_t st) {
+  for (int i = 0; i < f.n_row_cls; i++) {
+    const FftClass &c = f.row_cls[i];
+    int r = RICK_ERR_INVALID_ARG;
+    if (precision == RICK_PREC_FP64) {
+      switch (c.log) {
+#define X(L) case L: r = launch_rows<double, L>(f, c, st); break;
+        RICK_FFT_SIZES(X)
 #undef X
-    }
-  } else {
-    switch (lx) {
-#define X(L) case L: return launch_rows<float, L>(f, cube, g, st);
-      RICK_FFT_SIZES(X)
+      }
+    } else {
+      switch (c.log) {
+#define X(L) case L: r = launch_rows<float, L>(f, c, st); break;
+        RICK_FFT_SIZES(X)
 #undef X
+      }
     }
+    RICK_TRY(r);
   }
-  return set_error(RICK_ERR_UNSUPPORTED, "sparse FFT: unsupported row length %d", g.nx);
+  return RICK_OK;
 }
 
-int sparse_fft_cols_image(int precision, FftScratch &f, const void *cube, const Geometry &g,
-                          const double *ltab, const double *mtab, double wmin, double wmax,
-                          double norm, int phase_on, double *img_re, double *img_im,
-                          cudaStream_t st) {
-  const int ly = ilog2(g.ny);
-  if (precision == RICK_PREC_FP64) {
-    switch (ly) {
-#define X(L)                                                                                   \
-  case L:                                                                                      \
-    return launch_cols<double, L>(f, cube, g, ltab, mtab, wmin, wmax, norm, phase_on, img_re, \
-                                  img_im, st);
-      RICK_FFT_SIZES(X)
+int sparse_fft_cols(const FftJobs &f, int precision, cudaStream_t st) {
+  for (int i = 0; i < f.n_col_cls; i++) {
+    const FftClass &c = f.col_cls[i];
+    int r = RICK_ERR_INVALID_ARG;
+    if (precision == RICK_PREC_FP64) {
+      switch (c.log) {
+#define X(L) case L: r = launch_cols<double, L>(f, c, st); break;
+        RICK_FFT_SIZES(X)
 #undef X
-    }
-  } else {
-    switch (ly) {
-#define X(L)                                                                                  \
-  case L:                                                                                     \
-    return launch_cols<float, L>(f, cube, g, ltab, mtab, wmin, wmax, norm, phase_on, img_re, \
-                                 img_im, st);
-      RICK_FFT_SIZES(X)
+      }
+    } else {
+      switch (c.log) {
+#define X(L) case L: r = launch_cols<float, L>(f, c, st); break;
+        RICK_FFT_SIZES(X)
 #undef X
+      }
     }
+    RICK_TRY(r);
   }
-  return set_error(RICK_ERR_UNSUPPORTED, "sparse FFT: unsupported column length %d", g.ny);
+  return RICK_OK;
 }
 
 }  // namespace rick

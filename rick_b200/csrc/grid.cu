@@ -4,7 +4,9 @@
 // cell of every row with two FP64 atomics straight into HBM.  Here a persistent
 // kernel takes work items (a bounded chunk of the binned records of one
 // 32x32 tile of one w-plane), accumulates their footprints in shared memory in
-// FP64, and writes the tile once: with plain coalesced stores when the tile is
+// the cube's type (FP64 for the plain form, FP32 for the mixed form; weights
+// and products are formed in FP64 either way), and writes the tile once: with
+// plain coalesced stores when the tile is
 // a single item, or with one atomic per non-zero cell when a dense tile was
 // split over several items.  The kernel weights follow w-stacking.cu:162-180:
 //   u_dist = j + 0.5 - pos_u, table index (int)(5*|u_dist + KernelLen|),
@@ -28,7 +30,119 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-// LPR lanes per record (a power of two >= w_support); 32/LPR records per warp step.
+// Records r0..r1 of tile (tx, ty) of plane w: footprints accumulated in the
+// shared tile (s_re, s_im, zeroed by the caller), then the tile written to the
+// cube and the rows/tile it touched marked.  LPR lanes per record (a power of
+// two >= w_support); 32/LPR records per warp step.
+template <typename OutT, int LPR>
+__device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32_t r0, uint32_t r1,
+                                          const Geometry &g, bool hi, const double *s_tab,
+                                          int ntab, int tx, int ty, int w, bool single,
+                                          int accumulate, typename Vec2<OutT>::type *__restrict__ cube,
+                                          uint32_t *__restrict__ rowmask,
+                                          uint32_t *__restrict__ tilemask, OutT *s_re,
+                                          OutT *s_im, uint32_t *s_rows) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned d = lane % LPR;                 // footprint column / row handled
+  const unsigned grp_base = lane - d;            // first lane of this record's group
+  constexpr int RPW = 32 / LPR;                  // records per warp step
+  constexpr int kWarps = kGridThreads / 32;
+  const double gnorm = kStd22 / kPi;             // w-stacking.cu:256
+  const int x0 = tx * kTile, y0 = ty * kTile;
+
+  // Footprints of the chunk's records into the shared tile.
+  for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
+    const uint32_t r = rb + lane / LPR;
+    const bool valid = r < r1;
+    RecF64 q;
+    if (valid) q = rec[r];
+    else { q.sre = q.sim = q.fu = q.fv = 0.0; q.gu = q.gv = -1000000; }
+    double wu = 0.0, wv = 0.0;
+    if (valid && (int)d < g.support) {
+      const double off = __dadd_rn((double)((int)d - g.half), 0.5);
+      const double ud = __dsub_rn(off, q.fu);  // == (j + 0.5) - pos_u exactly
+      const double vd = __dsub_rn(off, q.fv);
+      if (hi) {
+        wu = exp(-__dmul_rn(ud, ud) * kStd22);
+        wv = exp(-__dmul_rn(vd, vd) * kStd22);
+      } else {
+        const int jk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(ud, (double)g.half)));
+        const int kk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(vd, (double)g.half)));
+        // In range for positions >= 0; rows with u or v in (-dx, 0) would index
+        // past the table (the reference reads out of bounds there): clamp.
+        wu = s_tab[min(jk, ntab - 1)];
+        wv = s_tab[min(kk, ntab - 1)];
+      }
+    }
+    const int j = q.gu - g.half + (int)d;
+    const bool col_ok = valid && (int)d < g.support && j >= 0 && j < g.nx && j >= x0 && j < x0 + kTile;
+    if (rowmask && valid && d == 0) {
+      // grid rows of this tile the record's footprint reaches
+      const int lo = max(max(q.gv - g.half, 0), y0);
+      const int hi_r = min(min(q.gv + g.half, g.ny - 1), y0 + kTile - 1);
+      if (lo <= hi_r) {
+        const uint32_t span = (uint32_t)(hi_r - lo + 1);
+        const uint32_t bits = (span >= 32u ? 0xffffffffu : ((1u << span) - 1u)) << (lo - y0);
+        atomicOr(s_rows, bits);
+      }
+    }
+    const double su = hi ? gnorm * wu : wu;
+    for (int e = 0; e < g.support; e++) {
+      const double wve = __shfl_sync(kFull, wv, grp_base + e);
+      const int k = q.gv - g.half + e;
+      if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
+        const double cw = su * wve;
+        const int cell = (k - y0) * kPitch + (j - x0);
+        atomicAdd(&s_re[cell], (OutT)(q.sre * cw));
+        atomicAdd(&s_im[cell], (OutT)(q.sim * cw));
+      }
+    }
+  }
+  __syncthreads();
+
+  // Flush the tile (and the rows it touched).
+  if (rowmask && threadIdx.x == 0 && *s_rows) {
+    atomicOr(&rowmask[(uint64_t)w * g.nty + ty], *s_rows);
+    const int tmw = (g.ntx + 31) / 32;
+    atomicOr(&tilemask[((uint64_t)w * g.nty + ty) * tmw + (tx >> 5)], 1u << (tx & 31));
+  }
+  const uint64_t plane = (uint64_t)g.nx * g.ny;
+  for (int c = threadIdx.x; c < kTile * kTile; c += blockDim.x) {
+    const int y = c / kTile, x = c % kTile;
+    const int gy = y0 + y, gx = x0 + x;
+    if (gy >= g.ny || gx >= g.nx) continue;
+    const uint64_t idx = (uint64_t)w * plane + (uint64_t)gy * g.nx + gx;
+    const OutT vr = s_re[y * kPitch + x], vi = s_im[y * kPitch + x];
+    if (single) {
+      if (accumulate) {
+        auto o = cube[idx];
+        o.x += vr;
+        o.y += vi;
+        cube[idx] = o;
+      } else {
+        typename Vec2<OutT>::type o;
+        o.x = vr;
+        o.y = vi;
+        cube[idx] = o;
+      }
+    } else if (vr != (OutT)0 || vi != (OutT)0) {
+      atomicAdd(&cube[idx].x, vr);
+      atomicAdd(&cube[idx].y, vi);
+    }
+  }
+}
+
+// last bin b with item_off[b] <= item
+__device__ __forceinline__ uint32_t bin_of_item(const uint32_t *__restrict__ item_off,
+                                                uint32_t nbins, uint32_t item) {
+  uint32_t lo = 0, hi_b = nbins;
+  while (hi_b - lo > 1) {
+    const uint32_t mid = (lo + hi_b) >> 1;
+    if (item_off[mid] <= item) lo = mid; else hi_b = mid;
+  }
+  return lo;
+}
+
 template <typename OutT, int LPR>
 __global__ void __launch_bounds__(kGridThreads)
     k_grid_tiles(const RecF64 *__restrict__ rec, const uint32_t *__restrict__ bin_off,
@@ -37,20 +151,14 @@ __global__ void __launch_bounds__(kGridThreads)
                  uint64_t *__restrict__ counters,
                  typename Vec2<OutT>::type *__restrict__ cube, uint32_t *__restrict__ rowmask,
                  uint32_t *__restrict__ tilemask) {
-  __shared__ double s_re[kTile * kPitch];
-  __shared__ double s_im[kTile * kPitch];
+  __shared__ OutT s_re[kTile * kPitch];
+  __shared__ OutT s_im[kTile * kPitch];
   __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
   __shared__ uint32_t s_item, s_bin, s_first, s_nitems, s_rows;
 
   const int ntab = kIncreasePrecision * g.support;
   for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = table[t];
   const uint32_t total_items = item_off[nbins];
-  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const unsigned d = lane % LPR;                 // footprint column / row handled
-  const unsigned grp_base = lane - d;            // first lane of this record's group
-  constexpr int RPW = 32 / LPR;                  // records per warp step
-  constexpr int kWarps = kGridThreads / 32;
-  const double gnorm = kStd22 / kPi;             // w-stacking.cu:256
   const bool hi = (kernel == RICK_KERNEL_GAUSS_HI_PRECISION);
 
   for (;;) {
@@ -58,13 +166,7 @@ __global__ void __launch_bounds__(kGridThreads)
       const uint32_t item = (uint32_t)atomicAdd((unsigned long long *)&counters[kCntItemNext], 1ull);
       uint32_t bin = 0;
       if (item < total_items) {
-        // last bin b with item_off[b] <= item
-        uint32_t lo = 0, hi_b = nbins;
-        while (hi_b - lo > 1) {
-          const uint32_t mid = (lo + hi_b) >> 1;
-          if (item_off[mid] <= item) lo = mid; else hi_b = mid;
-        }
-        bin = lo;
+        bin = bin_of_item(item_off, nbins, item);
         s_first = item_off[bin];
         s_nitems = item_off[bin + 1] - item_off[bin];
       }
@@ -73,102 +175,86 @@ __global__ void __launch_bounds__(kGridThreads)
       s_rows = 0;
     }
     for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
-      s_re[c] = 0.0;
-      s_im[c] = 0.0;
+      s_re[c] = (OutT)0;
+      s_im[c] = (OutT)0;
     }
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= total_items) break;
     const uint32_t bin = s_bin;
     const uint32_t chunk = item - s_first;
-    const bool single = (s_nitems == 1);
     const int tx = (int)(bin % (uint32_t)g.ntx);
     const int ty = (int)((bin / (uint32_t)g.ntx) % (uint32_t)g.nty);
     const int w = (int)(bin / ((uint32_t)g.ntx * (uint32_t)g.nty));
-    const int x0 = tx * kTile, y0 = ty * kTile;
     const uint32_t r0 = bin_off[bin] + chunk * max_chunk;
     const uint32_t r1 = min(bin_off[bin + 1], r0 + max_chunk);
+    grid_item<OutT, LPR>(rec, r0, r1, g, hi, s_tab, ntab, tx, ty, w, s_nitems == 1, accumulate,
+                         cube, rowmask, tilemask, s_re, s_im, &s_rows);
+    __syncthreads();
+  }
+}
 
-    // Footprints of the chunk's records into the shared tile.
-    for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
-      const uint32_t r = rb + lane / LPR;
-      const bool valid = r < r1;
-      RecF64 q;
-      if (valid) q = rec[r];
-      else { q.sre = q.sim = q.fu = q.fv = 0.0; q.gu = q.gv = -1000000; }
-      double wu = 0.0, wv = 0.0;
-      if (valid && (int)d < g.support) {
-        const double off = __dadd_rn((double)((int)d - g.half), 0.5);
-        const double ud = __dsub_rn(off, q.fu);  // == (j + 0.5) - pos_u exactly
-        const double vd = __dsub_rn(off, q.fv);
-        if (hi) {
-          wu = exp(-__dmul_rn(ud, ud) * kStd22);
-          wv = exp(-__dmul_rn(vd, vd) * kStd22);
-        } else {
-          const int jk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(ud, (double)g.half)));
-          const int kk = (int)__dmul_rn((double)kIncreasePrecision, fabs(__dadd_rn(vd, (double)g.half)));
-          // In range for positions >= 0; rows with u or v in (-dx, 0) would index
-          // past the table (the reference reads out of bounds there): clamp.
-          wu = s_tab[min(jk, ntab - 1)];
-          wv = s_tab[min(kk, ntab - 1)];
-        }
+// The same over every job of a batch: the bins of all jobs are numbered
+// consecutively, so the work items are too; a block reloads the kernel table
+// when its next item belongs to another job.
+template <typename OutT, int LPR>
+__global__ void __launch_bounds__(kGridThreads)
+    k_grid_tiles_batch(const BatchJob *__restrict__ jobs, int njobs,
+                       const uint32_t *__restrict__ bin_base, const RecF64 *__restrict__ rec,
+                       const uint32_t *__restrict__ bin_off, const uint32_t *__restrict__ item_off,
+                       uint32_t nbins, uint32_t max_chunk, uint64_t *__restrict__ counters,
+                       uint32_t *__restrict__ rowmask, uint32_t *__restrict__ tilemask) {
+  __shared__ OutT s_re[kTile * kPitch];
+  __shared__ OutT s_im[kTile * kPitch];
+  __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
+  __shared__ uint32_t s_item, s_bin, s_first, s_nitems, s_rows;
+  __shared__ int s_job;
+
+  const uint32_t total_items = item_off[nbins];
+  int cur_job = -1;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t item = (uint32_t)atomicAdd((unsigned long long *)&counters[kCntItemNext], 1ull);
+      uint32_t bin = 0;
+      int job = 0;
+      if (item < total_items) {
+        bin = bin_of_item(item_off, nbins, item);
+        s_first = item_off[bin];
+        s_nitems = item_off[bin + 1] - item_off[bin];
+        job = batch_job_of(bin_base, njobs, bin);
       }
-      const int j = q.gu - g.half + (int)d;
-      const bool col_ok = valid && (int)d < g.support && j >= 0 && j < g.nx && j >= x0 && j < x0 + kTile;
-      if (rowmask && valid && d == 0) {
-        // grid rows of this tile the record's footprint reaches
-        const int lo = max(max(q.gv - g.half, 0), y0);
-        const int hi = min(min(q.gv + g.half, g.ny - 1), y0 + kTile - 1);
-        if (lo <= hi) {
-          const uint32_t span = (uint32_t)(hi - lo + 1);
-          const uint32_t bits = (span >= 32u ? 0xffffffffu : ((1u << span) - 1u)) << (lo - y0);
-          atomicOr(&s_rows, bits);
-        }
-      }
-      const double su = hi ? gnorm * wu : wu;
-      for (int e = 0; e < g.support; e++) {
-        const double wve = __shfl_sync(kFull, wv, grp_base + e);
-        const int k = q.gv - g.half + e;
-        if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
-          const double cw = su * wve;
-          const int cell = (k - y0) * kPitch + (j - x0);
-          atomicAdd(&s_re[cell], q.sre * cw);
-          atomicAdd(&s_im[cell], q.sim * cw);
-        }
-      }
+      s_item = item;
+      s_bin = bin;
+      s_job = job;
+      s_rows = 0;
+    }
+    for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
+      s_re[c] = (OutT)0;
+      s_im[c] = (OutT)0;
     }
     __syncthreads();
-
-    // Flush the tile (and the rows it touched).
-    if (rowmask && threadIdx.x == 0 && s_rows) {
-      atomicOr(&rowmask[(uint64_t)w * g.nty + ty], s_rows);
-      const int tmw = (g.ntx + 31) / 32;
-      atomicOr(&tilemask[((uint64_t)w * g.nty + ty) * tmw + (tx >> 5)], 1u << (tx & 31));
+    const uint32_t item = s_item;
+    if (item >= total_items) break;
+    const int j = s_job;
+    const BatchJob &J = jobs[j];
+    const Geometry g = J.g;
+    const int ntab = kIncreasePrecision * g.support;
+    if (j != cur_job) {  // block-uniform
+      for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = J.table[t];
+      cur_job = j;
+      __syncthreads();
     }
-    const uint64_t plane = (uint64_t)g.nx * g.ny;
-    for (int c = threadIdx.x; c < kTile * kTile; c += blockDim.x) {
-      const int y = c / kTile, x = c % kTile;
-      const int gy = y0 + y, gx = x0 + x;
-      if (gy >= g.ny || gx >= g.nx) continue;
-      const uint64_t idx = (uint64_t)w * plane + (uint64_t)gy * g.nx + gx;
-      const double vr = s_re[y * kPitch + x], vi = s_im[y * kPitch + x];
-      if (single) {
-        if (accumulate) {
-          auto o = cube[idx];
-          o.x += (OutT)vr;
-          o.y += (OutT)vi;
-          cube[idx] = o;
-        } else {
-          typename Vec2<OutT>::type o;
-          o.x = (OutT)vr;
-          o.y = (OutT)vi;
-          cube[idx] = o;
-        }
-      } else if (vr != 0.0 || vi != 0.0) {
-        atomicAdd(&cube[idx].x, (OutT)vr);
-        atomicAdd(&cube[idx].y, (OutT)vi);
-      }
-    }
+    const uint32_t bin = s_bin;
+    const uint32_t lbin = bin - J.bin_base;
+    const uint32_t chunk = item - s_first;
+    const int tx = (int)(lbin % (uint32_t)g.ntx);
+    const int ty = (int)((lbin / (uint32_t)g.ntx) % (uint32_t)g.nty);
+    const int w = (int)(lbin / ((uint32_t)g.ntx * (uint32_t)g.nty));
+    const uint32_t r0 = bin_off[bin] + chunk * max_chunk;
+    const uint32_t r1 = min(bin_off[bin + 1], r0 + max_chunk);
+    grid_item<OutT, LPR>(rec, r0, r1, g, J.kernel == RICK_KERNEL_GAUSS_HI_PRECISION, s_tab, ntab,
+                         tx, ty, w, s_nitems == 1, 0, (typename Vec2<OutT>::type *)J.cube,
+                         rowmask + J.mask_base, tilemask + J.tile_base, s_re, s_im, &s_rows);
     __syncthreads();
   }
 }
@@ -176,26 +262,46 @@ __global__ void __launch_bounds__(kGridThreads)
 // Tiles split over several work items receive their parts with atomics, so
 // they must start at zero when the cube is not cleared as a whole.
 template <typename OutT>
+__device__ __forceinline__ void zero_tile(const Geometry &g, uint64_t b,
+                                          typename Vec2<OutT>::type *__restrict__ cube) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t plane = (uint64_t)g.nx * g.ny;
+  const int tx = (int)(b % (uint32_t)g.ntx);
+  const int ty = (int)((b / (uint32_t)g.ntx) % (uint32_t)g.nty);
+  const int w = (int)(b / ((uint64_t)g.ntx * g.nty));
+  const int gx = tx * kTile + (int)lane;
+  if (gx >= g.nx) return;
+  typename Vec2<OutT>::type z;
+  z.x = 0;
+  z.y = 0;
+  for (int y = 0; y < kTile; y++) {
+    const int gy = ty * kTile + y;
+    if (gy < g.ny) cube[(uint64_t)w * plane + (uint64_t)gy * g.nx + gx] = z;
+  }
+}
+
+template <typename OutT>
 __global__ void k_zero_split_tiles(const uint32_t *__restrict__ item_off, uint32_t nbins, Geometry g,
                                    typename Vec2<OutT>::type *__restrict__ cube) {
-  const unsigned lane = threadIdx.x & 31u;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
-  const uint64_t plane = (uint64_t)g.nx * g.ny;
   for (uint64_t b = warp; b < nbins; b += nwarps) {
     if (item_off[b + 1] - item_off[b] <= 1) continue;
-    const int tx = (int)(b % (uint32_t)g.ntx);
-    const int ty = (int)((b / (uint32_t)g.ntx) % (uint32_t)g.nty);
-    const int w = (int)(b / ((uint64_t)g.ntx * g.nty));
-    const int gx = tx * kTile + (int)lane;
-    if (gx >= g.nx) continue;
-    typename Vec2<OutT>::type z;
-    z.x = 0;
-    z.y = 0;
-    for (int y = 0; y < kTile; y++) {
-      const int gy = ty * kTile + y;
-      if (gy < g.ny) cube[(uint64_t)w * plane + (uint64_t)gy * g.nx + gx] = z;
-    }
+    zero_tile<OutT>(g, b, cube);
+  }
+}
+
+template <typename OutT>
+__global__ void k_zero_split_tiles_batch(const BatchJob *__restrict__ jobs, int njobs,
+                                         const uint32_t *__restrict__ bin_base,
+                                         const uint32_t *__restrict__ item_off, uint32_t nbins) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  for (uint64_t b = warp; b < nbins; b += nwarps) {
+    if (item_off[b + 1] - item_off[b] <= 1) continue;
+    const int j = batch_job_of(bin_base, njobs, (uint32_t)b);
+    const Geometry g = jobs[j].g;
+    zero_tile<OutT>(g, b - jobs[j].bin_base, (typename Vec2<OutT>::type *)jobs[j].cube);
   }
 }
 
@@ -245,6 +351,40 @@ int zero_split_tiles(const Geometry &g, int precision, Scratch &s, void *cube, c
                                                                    (float2 *)cube);
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
+}
+
+namespace {
+
+template <typename OutT>
+int launch_grid_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cudaStream_t st) {
+  const int sms = num_sms();
+  const uint32_t nbins = b.total_bins;
+  const int zblocks = (int)std::min<uint64_t>(((uint64_t)nbins * 32 + 255) / 256, (uint64_t)sms * 16);
+  RICK_LAUNCHED();
+  k_zero_split_tiles_batch<OutT><<<std::max(zblocks, 1), 256, 0, st>>>(b.jobs, b.njobs,
+                                                                      b.u.bin_base, s.item_off,
+                                                                      nbins);
+  RICK_CUDA(cudaGetLastError());
+  const int blocks = sms * std::max(1, b.grid_blocks_per_sm);
+  RICK_LAUNCHED();
+  if (b.max_support <= 8)
+    k_grid_tiles_batch<OutT, 8><<<blocks, kGridThreads, 0, st>>>(
+        b.jobs, b.njobs, b.u.bin_base, s.records, s.bin_count, s.item_off, nbins, max_chunk,
+        s.counters, b.rowmask, b.tilemask);
+  else
+    k_grid_tiles_batch<OutT, 16><<<blocks, kGridThreads, 0, st>>>(
+        b.jobs, b.njobs, b.u.bin_base, s.records, s.bin_count, s.item_off, nbins, max_chunk,
+        s.counters, b.rowmask, b.tilemask);
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
+}  // namespace
+
+int grid_tiles_batch(const BatchLaunch &b, int precision, Scratch &s, uint32_t max_chunk,
+                     cudaStream_t st) {
+  if (precision == RICK_PREC_FP64) return launch_grid_batch<double>(b, s, max_chunk, st);
+  return launch_grid_batch<float>(b, s, max_chunk, st);
 }
 
 }  // namespace rick

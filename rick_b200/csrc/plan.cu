@@ -146,9 +146,13 @@ struct rick_plan {
   cudaEvent_t ev[RICK_NUM_STAGES + 1] = {};
   bool ran[RICK_NUM_STAGES] = {};
   cudaEvent_t ev_fft0 = nullptr, ev_phase0 = nullptr;
-  // sparse-aware FFT (power-of-two axes)
+  // sparse-aware FFT (power-of-two axes): the plan is a set of one job
   bool sparse = false;
   FftScratch f{};
+  FftJobs fj{};
+  BatchJob *d_job = nullptr;      // [1]
+  uint32_t *d_fft_tabs = nullptr; // fft_units [2], col_jobs [1], col_units [2]
+  uint64_t *d_mask_base = nullptr;  // [2]
 };
 
 namespace {
@@ -276,6 +280,30 @@ int mark(rick_plan *p, cudaEvent_t e, cudaStream_t st) {
   return RICK_OK;
 }
 
+// The plan as the one job of its FFT stages (fft.cu): geometry, cube, buffers
+// and twiddles; the image fields are filled per call.
+BatchJob plan_job(const rick_plan *p) {
+  BatchJob j{};
+  j.g = p->g;
+  j.kernel = p->d.kernel;
+  int lx = 0, ly = 0;
+  while ((1 << lx) < p->d.grid_size_x) lx++;
+  while ((1 << ly) < p->d.grid_size_y) ly++;
+  j.logx = lx;
+  j.logy = ly;
+  j.nchan = p->d.freq_per_chan;
+  j.npol = p->d.polarizations;
+  j.cube = p->cube;
+  j.blocked = p->f.blocked;
+  j.table = p->s.table;
+  const bool f64 = p->d.precision == RICK_PREC_FP64;
+  j.tw_x = f64 ? (const void *)p->f.tw_x64 : (const void *)p->f.tw_x32;
+  j.tw_y = f64 ? (const void *)p->f.tw_y64 : (const void *)p->f.tw_y32;
+  j.ltab = p->d_lm;
+  j.mtab = p->d_lm + p->d.grid_size_x;
+  return j;
+}
+
 int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
                    const double *ww, const float *weight, const float *vis_re, const float *vis_im,
                    int select, int accumulate, double dx, double dw, cudaStream_t st,
@@ -323,15 +351,26 @@ int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const doub
   RICK_TRY(plan_grid_impl(p, nrows, uu, vv, ww, weight, vis_re, vis_im, select, 0,
                           1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, st, true));
   RICK_TRY(mark(p, p->ev_fft0, st));
-  RICK_TRY(sparse_row_list(p->f, p->g, st));
-  RICK_TRY(sparse_fft_rows(p->d.precision, p->f, p->cube, p->g, st));
-  RICK_TRY(mark(p, p->ev[5], st));
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
+  BatchJob j = plan_job(p);
+  j.nrows = nrows;
+  j.wmin = wmin;
+  j.dw_phase = (wmax - wmin) / (double)p->d.num_w_planes;  // phase_correction.cu:100-102
+  j.dwnorm = j.dw_phase / (wmax - wmin);
+  j.norm = 1.0 / (double)((long long)nx * ny);  // fourier_transform.c:24
+  j.phase_on = p->d.phase_on;
+  j.img_re = img_re;
+  j.img_im = img_im;
+  // from pageable memory: the call returns once `j` has been staged
+  RICK_CUDA(cudaMemcpyAsync(p->d_job, &j, sizeof(j), cudaMemcpyHostToDevice, st));
+  p->fj.one = &j;
+  RICK_TRY(sparse_fft_lists(p->fj, st));
+  RICK_TRY(sparse_fft_rows(p->fj, p->d.precision, st));
+  RICK_TRY(mark(p, p->ev[5], st));
   RICK_TRY(ensure_lm(p, nx, ny, nx, ny, resolution, st));
   RICK_TRY(mark(p, p->ev_phase0, st));
-  const double norm = 1.0 / (double)((long long)nx * ny);  // fourier_transform.c:24
-  RICK_TRY(sparse_fft_cols_image(p->d.precision, p->f, p->cube, p->g, p->d_lm, p->d_lm + nx, wmin,
-                                 wmax, norm, p->d.phase_on, img_re, img_im, st));
+  RICK_TRY(sparse_fft_cols(p->fj, p->d.precision, st));
+  p->fj.one = nullptr;
   RICK_TRY(mark(p, p->ev[6], st));
   p->ran[4] = p->ran[5] = true;
   p->cube_state = kCubeSparse;
@@ -393,8 +432,10 @@ int rick_plan_footprint(const rick_plan_desc *desc, uint64_t *bytes) {
   const uint64_t nbins = nw * ((nx + kTile - 1) / kTile) * ((ny + kTile - 1) / kTile);
   const uint64_t vb = desc->precision == RICK_PREC_FP64 ? 8 : 4;
   uint64_t b = 2 * nw * nx * ny * vb;                      // cube
-  if (sparse_fft_supported((int)nx, (int)ny)) b *= 2;      // + column-blocked planes
-  b += std::max<uint64_t>(b / 4, 512ull << 20);            // FFT work (upper bound)
+  if (sparse_fft_supported((int)nx, (int)ny))
+    b *= 2;                                                // + column-blocked planes
+  else
+    b += std::max<uint64_t>(b / 4, 512ull << 20);          // cuFFT work (upper bound)
   b += 4 * (nbins + 1) * 4 + 4 * scan_tmp_words(nbins + 1);  // bins, items, cursor, scan
   b += 4 * desc->max_rows * sizeof(RecF64);                // records
   b += (nx + ny) * 8 + 64;
@@ -476,8 +517,35 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
       free(t64);
       free(t32);
     }
+    A((void **)&p->d_job, sizeof(BatchJob));
+    A((void **)&p->d_fft_tabs, 8 * sizeof(uint32_t));
+    A((void **)&p->d_mask_base, 2 * sizeof(uint64_t));
+    if (st == RICK_OK) {
+      FftJobs &fj = p->fj;
+      BatchJob hj = plan_job(p);
+      uint32_t tabs[8] = {};
+      fft_classes(&hj, 1, fj, tabs + 2, tabs + 3);
+      const uint64_t mb[2] = {0, (uint64_t)desc->num_w_planes * p->g.nty};
+      fj.jobs = p->d_job;
+      fj.njobs = 1;
+      fj.fft_units = p->d_fft_tabs;
+      fj.col_jobs = p->d_fft_tabs + 2;
+      fj.col_units = p->d_fft_tabs + 3;
+      fj.mask_base = p->d_mask_base;
+      fj.total_mask_words = mb[1];
+      fj.total_count_words = 1 + desc->num_w_planes;
+      fj.rowmask = p->f.rowmask;
+      fj.tilemask = p->f.tilemask;
+      fj.rowlist = p->f.rowlist;
+      fj.counts = p->f.counts;
+      cudaError_t e = cudaMemcpy(p->d_fft_tabs, tabs, sizeof(tabs), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(p->d_mask_base, mb, sizeof(mb), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) st = cuda_status(e, "cudaMemcpy(fft tables)", __FILE__, __LINE__);
+    }
   }
-  if (st == RICK_OK) st = choose_fft(p);
+  // the sparse-aware path needs no cuFFT plan: the stage API creates it (and its
+  // work area) on first use
+  if (st == RICK_OK && !p->sparse) st = choose_fft(p);
   if (st != RICK_OK) {
     rick_plan_destroy(p);
     return st;
@@ -495,7 +563,7 @@ int rick_plan_destroy(rick_plan *p) {
                   p->s.counters, p->s.records, p->s.table, p->d_lm, p->fft_work, p->h_rows_d,
                   p->d_img, p->d_stage, p->f.rowmask, p->f.rowlist, p->f.counts,
                   p->f.tw_x64, p->f.tw_y64, p->f.tw_x32, p->f.tw_y32, p->f.blocked,
-                  p->f.tilemask};
+                  p->f.tilemask, p->d_job, p->d_fft_tabs, p->d_mask_base};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->h_lm) cudaFreeHost(p->h_lm);

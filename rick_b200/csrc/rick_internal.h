@@ -93,6 +93,73 @@ struct FftScratch {
   void *blocked = nullptr;      // row-transformed planes, column-blocked (cube-sized)
 };
 
+// One job of a batch (batch.cu), as the batch kernels see it: the job's
+// geometry, its inputs and outputs, and where its slices of the batch-wide
+// arrays start.  Work units of every stage are numbered across all jobs; a
+// kernel finds the job of a unit by binary search over the unit bases.
+struct BatchJob {
+  Geometry g;
+  int kernel;                      // RICK_KERNEL_*
+  int logx, logy;                  // log2 of the axes (sparse FFT sizes)
+  uint64_t nrows;                  // rows of the job
+  uint32_t nchan, npol;
+  uint32_t bin_base;               // first global bin (nw*nty*ntx bins per job)
+  uint32_t counts_base;            // first word of the job's [1 + nw] row counts
+  uint64_t mask_base;              // first word of the job's row mask [nw * nty]
+  uint64_t tile_base;              // first word of the job's tile bitmap [nw * nty * tmw]
+  uint64_t list_base;              // first entry of the job's row list [nw * ny]
+  const double *uu, *vv, *ww;      // rows (device)
+  const float *weight, *vis_re, *vis_im;
+  void *cube;                      // [nw][ny][nx] complex (T)
+  void *blocked;                   // column-blocked row transforms (cube-sized)
+  const double *table;             // 1-D kernel table (5*support)
+  const void *tw_x, *tw_y;         // per-pass twiddles of the two axes (T)
+  const double *ltab, *mtab;       // phase tables (nx, ny)
+  double wmin, dw_phase, dwnorm, norm;
+  int phase_on;
+  double *img_re, *img_im;         // image (device, [ny][nx])
+};
+
+// Batch-wide unit bases of the binning and gridding stages (device arrays of
+// njobs + 1 entries, exclusive prefix sums).
+struct BatchUnits {
+  const uint64_t *row_units;   // 32-row binning units per job
+  const uint32_t *bin_base;    // bins per job (== BatchJob::bin_base, plus the total)
+};
+
+// FFT stages of a set of jobs (a plan is a set of one): jobs sorted by logx, so
+// that the jobs of one row-FFT length are contiguous; the column pass lists them
+// grouped by logy.  One launch per FFT length present.
+struct FftClass {
+  int log;         // log2 of the FFT length
+  int lo, hi;      // jobs[lo..hi) (row pass) or col_jobs[lo..hi) (column pass)
+  uint32_t units;  // column groups of the class (column pass)
+};
+struct FftJobs {
+  const BatchJob *jobs = nullptr;    // device [njobs]
+  int njobs = 0;
+  uint32_t *fft_units = nullptr;     // device [njobs + 1], row-pass units (filled on the device)
+  const uint32_t *col_jobs = nullptr;   // device [njobs]
+  const uint32_t *col_units = nullptr;  // device [njobs + 1], in col_jobs order
+  const uint64_t *mask_base = nullptr;  // device [njobs + 1], row-mask words per job
+  uint64_t total_mask_words = 0;
+  uint32_t total_count_words = 0;
+  uint32_t *rowmask = nullptr, *tilemask = nullptr, *rowlist = nullptr, *counts = nullptr;
+  int n_row_cls = 0, n_col_cls = 0;
+  FftClass row_cls[8], col_cls[8];
+  int cols_pp = 2;                   // planes per column-pass iteration allowed (1 or 2)
+  // a set of one job (a plan): its host copy; the FFT kernels then take the
+  // job as kernel parameters instead of reading the device table
+  const BatchJob *one = nullptr;
+};
+
+// Rows (columns) one block of the row (column) pass transforms at length 2^logn:
+// a row takes 2^logn / 8 threads, a block max(256, 2^logn / 8).
+__host__ __device__ inline int fft_rows_per_block(int logn) {
+  const int g = (1 << logn) / 8;
+  return (g > 256 ? g : 256) / g;
+}
+
 enum Counter : int {
   kCntDropped = 0,    // rows outside the cube / sector
   kCntGridded = 1,    // rows that produced records
@@ -120,13 +187,6 @@ int zero_split_tiles(const Geometry &g, int precision, Scratch &s, void *cube, c
 // Sparse-aware FFT (fft.cu).
 bool sparse_fft_supported(int nx, int ny);
 void make_twiddles(int n, double2 *t64, float2 *t32);
-int sparse_row_list(FftScratch &f, const Geometry &g, cudaStream_t st);
-int sparse_fft_rows(int precision, FftScratch &f, void *cube, const Geometry &g,
-                    cudaStream_t st);
-int sparse_fft_cols_image(int precision, FftScratch &f, const void *cube, const Geometry &g,
-                          const double *ltab, const double *mtab, double wmin, double wmax,
-                          double norm, int phase_on, double *img_re, double *img_im,
-                          cudaStream_t st);
 void phase_tables(int xaxis, int yaxis, int xaxistot, int yaxistot, double resolution,
                   double *l, double *m);
 int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, const double *ltab,
@@ -135,6 +195,47 @@ int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, con
 int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *tmp,
                        cudaStream_t st);
 uint64_t scan_tmp_words(uint64_t n);
+
+#ifdef __CUDACC__
+// Index j of the job that owns unit x: the last j with base[j] <= x, for an
+// exclusive prefix base[0..njobs] with x < base[njobs].
+template <typename U>
+__device__ __forceinline__ int batch_job_of(const U *__restrict__ base, int njobs, U x) {
+  int lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+#endif
+
+// Batch stages: every job of the batch in one launch per kernel.
+struct BatchLaunch {
+  const BatchJob *jobs;    // device [njobs]
+  int njobs;
+  BatchUnits u;
+  uint64_t total_row_units;
+  uint32_t total_bins;
+  int max_nv;              // largest nchan*npol
+  bool v4;                 // every job allows 16-byte sample loads
+  int max_support;
+  uint32_t *rowmask, *tilemask;  // batch-wide arrays
+  int grid_blocks_per_sm;  // gridder occupancy (tuned)
+};
+int bin_rows_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cudaStream_t st);
+int grid_tiles_batch(const BatchLaunch &b, int precision, Scratch &s, uint32_t max_chunk,
+                     cudaStream_t st);
+
+// The sparse-aware FFT stages (fft.cu) of a set of jobs.  fft_classes fills the
+// classes and the host copies of col_jobs / col_units (njobs and njobs + 1
+// entries) from the host copy of the jobs (sorted by logx).
+void fft_classes(const BatchJob *host_jobs, int njobs, FftJobs &f, uint32_t *col_jobs,
+                 uint32_t *col_units);
+int sparse_fft_lists(const FftJobs &f, cudaStream_t st);  // row lists and row-pass units
+int sparse_fft_rows(const FftJobs &f, int precision, cudaStream_t st);
+int sparse_fft_cols(const FftJobs &f, int precision, cudaStream_t st);
 
 int num_sms();
 

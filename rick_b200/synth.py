@@ -236,3 +236,49 @@ def to_numpy(obs: Observation) -> Observation:
     return dataclasses.replace(obs, uu=cv(obs.uu), vv=cv(obs.vv), ww=cv(obs.ww),
                                weights=cv(obs.weights), vis_re=cv(obs.vis_re),
                                vis_im=cv(obs.vis_im))
+
+
+# ---- batched snapshot imaging: many small independent jobs ------------------
+
+@dataclasses.dataclass
+class BatchJobSpec:
+    """One job of the batched-snapshot workload: its observation and image shape."""
+    obs: Observation
+    grid: int
+    w_planes: int
+    kernel: str
+    w_support: int
+
+    @property
+    def nvis(self) -> int:
+        return int(self.obs.meta["Nvis"])
+
+
+def snapshot_jobs(n_jobs: int = 256, seed: int = 4242, device: str = "cpu",
+                  vis_range=(1e4, 1e7), grids=(256, 512, 1024, 2048), planes=(4, 16),
+                  chans=(1, 4), kernel: str = "kaiser_bessel", w_support: int = 7,
+                  scale: float = 1.0) -> list[BatchJobSpec]:
+    """ALMA-like compact-array snapshots: 43 antennas within 500 m at latitude
+    -23 deg, declination uniform in [-60, +20] deg, 2 s integrations, 1-4
+    channels across 99.5-100.5 GHz, 2 polarisations, 5-50 log-normal point
+    sources in a 0.01 deg field plus noise 0.1.  Visibility counts log-uniform
+    in ``vis_range`` (times ``scale``), grids drawn from ``grids``, w-planes
+    uniform in ``planes``.  Seeded per job."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    nbl = 43 * 42 // 2
+    for j in range(n_jobs):
+        nvis = float(np.exp(rng.uniform(np.log(vis_range[0]), np.log(vis_range[1])))) * scale
+        nchan = int(rng.integers(chans[0], chans[1] + 1))
+        npol = 2
+        rows = max(nbl, int(nvis / (nchan * npol)))
+        ntimes = max(1, int(round(rows / nbl)))
+        dt = 2.0
+        cfg = ObsConfig(f"snap{j}", "compact", 43, 500.0, -23.0,
+                        float(rng.uniform(-60.0, 20.0)), ntimes * dt / 3600.0, dt, nchan,
+                        99.5e9, 100.5e9, npol, int(rng.integers(5, 51)), "lognormal", 0.01, 0.1,
+                        int(rng.choice(grids)), int(rng.integers(planes[0], planes[1] + 1)),
+                        kernel, w_support)
+        obs = make_observation(cfg, seed=seed * 1000 + j, device=device)
+        specs.append(BatchJobSpec(obs, cfg.grid, cfg.w_planes, kernel, w_support))
+    return specs
