@@ -71,6 +71,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-snapshot leg (256 small jobs, one graph)")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batched-snapshot leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--served-requests", type=int, default=300)
+    ap.add_argument("--served-rates", type=float, nargs="+", default=[250.0, 500.0, 1000.0, 0.0],
+                    help="arrival rates (jobs/s) of the served-stream leg; 0 = all at once")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched-snapshot leg and print its line (profiling)")
     return ap.parse_args()
@@ -341,7 +345,12 @@ def run_ours(args):
         "cpu_baseline": cpu,
     }
     if not args.no_batched and world == 1:
-        line["batched"] = run_batched(args, dev, stream)
+        ctx, line["batched"] = run_batched(args, dev, stream)
+        if not args.no_served:
+            big = {"grid": nx, "w_planes": nw, "w_support": cfg.w_support, "kernel": cfg.kernel,
+                   "rows_n": n, "nchan": nchan, "npol": npol, "rows": rows, "res": res,
+                   "wmin": wmin, "wmax": wmax, "nvis": nvis, "alone_ms": ms64}
+            line["served"] = run_served(args, dev, stream, ctx, big)
     if rank == 0:
         line["clocks"] = clocks.summary()
         print(json.dumps(line), flush=True)
@@ -403,7 +412,7 @@ def run_batched(args, dev, stream):
     del imgs
 
     # every job alone, FP64 plain form, one plan per job (created untimed)
-    alone_ms, errs = 0.0, []
+    alone_ms, errs, alone_each = 0.0, [], []
     for sp, (job, mimg) in zip(specs, zip(jobs, mixed_imgs)):
         o, g = sp.obs, sp.grid
         geom = R.Geometry(g, g, sp.w_planes, sp.w_support, sp.kernel, "fp64")
@@ -418,9 +427,11 @@ def run_batched(args, dev, stream):
             e1.record(stream)
             torch.cuda.synchronize()
             alone_ms += e0.elapsed_time(e1)
+            alone_each.append(e0.elapsed_time(e1))
             den = torch.linalg.vector_norm(img)
             errs.append(float(torch.linalg.vector_norm(mimg - img) / den) if den > 0 else 0.0)
-    return {"workload": f"{len(specs)} ALMA-like snapshot jobs, {total_vis:.3e} vis, grids "
+    ctx = {"specs": specs, "jobs": jobs, "alone_ms": alone_each}
+    return ctx, {"workload": f"{len(specs)} ALMA-like snapshot jobs, {total_vis:.3e} vis, grids "
                         f"256^2-2048^2, 4-16 w-planes, Kaiser-Bessel support 7",
             "visibilities": total_vis, "jobs": len(specs),
             "grids": {str(g): sum(1 for sp in specs if sp.grid == g) for g in (256, 512, 1024, 2048)},
@@ -435,6 +446,78 @@ def run_batched(args, dev, stream):
             "batched_mixed_over_fp64_alone": alone_ms / ms,
             "rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
             "generate_s": gen_s}
+
+
+def run_served(args, dev, stream, ctx, big):
+    """Served imaging stream: Poisson arrivals at swept rates, jobs drawn from the
+    snapshot mix plus 5% LOFAR-sized jobs (the headline job: 4096^2 x 32, 1.3e9
+    vis), device-resident rows, admission by HBM footprint under a 150 GB
+    budget, continuous batching on 2 streams.  Reports p50/p99 latency and
+    sustained vis/s per rate against imaging the same requests one at a time in
+    the FP64 plain form."""
+    import torch
+    import rick_b200 as R
+
+    specs, alone_ms = ctx["specs"], ctx["alone_ms"]
+    rng = np.random.default_rng(777)
+    budget = 150 * 10**9
+
+    def request(k_big):
+        if k_big:
+            g = big["grid"]
+            img = torch.empty(2 * g * g, dtype=torch.float64, device=dev)
+            job = R.Job(R.Geometry(g, g, big["w_planes"], big["w_support"], big["kernel"], "mixed"),
+                        big["rows_n"], big["nchan"], big["npol"], big["rows"], big["res"],
+                        big["wmin"], big["wmax"], img[: g * g], img[g * g:], R.ROWS_SECTOR0)
+            return job, big["nvis"], big["alone_ms"], img
+        i = int(rng.integers(len(specs)))
+        sp, base = specs[i], ctx["jobs"][i]
+        g = sp.grid
+        img = torch.empty(2 * g * g, dtype=torch.float64, device=dev)
+        job = R.Job(R.Geometry(g, g, sp.w_planes, sp.w_support, sp.kernel, "mixed"), base.nrows,
+                    base.freq_per_chan, base.polarizations, base.rows, base.resolution,
+                    base.wmin, base.wmax, img[: g * g], img[g * g:])
+        return job, sp.nvis, alone_ms[i], img
+
+    out = {"workload": "Poisson arrivals of snapshot jobs plus 5% LOFAR-sized jobs "
+                       "(4096^2 x 32, 1.3e9 vis), mixed form, budget 150 GB, 3 streams; rate 0 = all at once",
+           "budget_gb": budget / 1e9, "rates": []}
+    n_req = args.served_requests
+    torch.cuda.empty_cache()  # the pool reserves the whole budget up front
+    with R.Server("mixed", device=dev.index or 0, hbm_budget=budget, max_batch_jobs=64,
+                  streams=3) as srv:
+        warm = [request(False) for _ in range(8)] + [request(True)]
+        for t in [srv.submit(j) for j, _, _, _ in warm]:
+            srv.wait(t)
+        for rate in args.served_rates:
+            reqs = [request(rng.random() < 0.05) for _ in range(n_req)]
+            # rate 0: every request at once (the server's capacity)
+            arrivals = (np.cumsum(rng.exponential(1.0 / rate, n_req)) if rate > 0
+                        else np.zeros(n_req))
+            torch.cuda.synchronize()
+            tickets = []
+            t0 = time.perf_counter()
+            for (job, _, _, _), at in zip(reqs, arrivals):
+                while time.perf_counter() - t0 < at:
+                    pass
+                tickets.append(srv.submit(job))
+            res = [srv.wait(t) for t in tickets]
+            span = time.perf_counter() - t0
+            st = srv.stats()
+            lat = [r["latency_ms"] for r in res]
+            vis = sum(v for _, v, _, _ in reqs)
+            alone = sum(a for _, _, a, _ in reqs)
+            out["rates"].append({
+                "rate_jobs_per_s": rate, "jobs": n_req, "big_jobs": sum(1 for j in reqs if j[1] == big["nvis"]),
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "sustained_vis_per_s": vis / span,
+                "fp64_alone_vis_per_s": vis / (alone * 1e-3),
+                "served_over_fp64_alone_offered": (vis / span) / (vis / (alone * 1e-3)),
+                "mean_batch_jobs": float(np.mean([r["batch_jobs"] for r in res])),
+                "peak_gb": st["peak_bytes"] / 1e9})
+            del reqs
+    # capacity: the highest rate's sustained throughput is bounded by the offered load
+    return out
 
 
 def _threads():
@@ -555,7 +638,7 @@ def main():
         import torch
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
-        print(json.dumps(run_batched(args, dev, torch.cuda.current_stream(dev))), flush=True)
+        print(json.dumps(run_batched(args, dev, torch.cuda.current_stream(dev))[1]), flush=True)
     else:
         run_ours(args)
 

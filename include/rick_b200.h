@@ -253,6 +253,53 @@ int rick_batch_kernels_per_run(rick_batch *batch, uint32_t *kernels);
 int rick_batch_get_stats(rick_batch *batch, rick_plan_stats *stats);
 int rick_batch_destroy(rick_batch *batch);
 
+/* ---- 5. Served imaging ---------------------------------------------------
+ * No counterpart in the reference.  A request loop with continuous batching:
+ * jobs are submitted from any thread as they arrive; a scheduler thread admits
+ * waiting jobs (oldest first) while their HBM footprint fits the budget,
+ * launches them as one batch on a free stream, and keeps admitting while
+ * earlier batches run, so batches overlap on the device.  Job rows and images
+ * are device pointers owned by the caller and must stay valid until the job's
+ * wait returns.  Each job's image is the same as imaging it alone (within the
+ * precision's tolerance: tiles split over work items add in any order). */
+typedef struct rick_server rick_server;
+
+typedef struct rick_server_desc {
+  int device;
+  int precision;          /* RICK_PREC_* */
+  uint64_t hbm_budget;    /* bytes of working memory the admitted jobs may hold */
+  int max_batch_jobs;     /* jobs per launched batch at most */
+  int streams;            /* batches on the device at once at most */
+  uint64_t solo_vis;      /* jobs with at least this many visibilities run as a batch of their
+                             own, beside the small-job batches (0: 5e7) */
+} rick_server_desc;
+
+typedef struct rick_job_result {
+  int status;
+  double queue_ms;        /* submit -> launch */
+  double latency_ms;      /* submit -> image complete on the device */
+  uint64_t batch_id;
+  uint32_t batch_jobs;    /* jobs of the batch it ran in */
+} rick_job_result;
+
+typedef struct rick_server_stats {
+  uint64_t jobs_submitted, jobs_done, vis_done, batches;
+  uint64_t bytes_in_use, peak_bytes, jobs_waiting;
+} rick_server_stats;
+
+/* Reserves the whole budget in the server's stream-ordered pool at creation
+ * (RICK_ERR_NOT_ENOUGH_MEM if the device cannot hold it). */
+int rick_server_create(rick_server **server, const rick_server_desc *desc);
+/* Queues one job; RICK_ERR_BUDGET when the job alone exceeds the budget. */
+int rick_server_submit(rick_server *server, const rick_job_desc *job, uint64_t *ticket);
+/* Waits for the job (timeout_ms < 0: no limit; RICK_ERR_CANCELLED on timeout)
+ * and returns its status; the ticket is released. */
+int rick_server_wait(rick_server *server, uint64_t ticket, double timeout_ms,
+                     rick_job_result *result);
+int rick_server_get_stats(rick_server *server, rick_server_stats *stats);
+/* Finishes every submitted job, then releases the server. */
+int rick_server_destroy(rick_server *server);
+
 /* Names of the kernels this library launches, and how many launches it has
  * issued in this process (for launch accounting). */
 int rick_kernel_names(const char **names, int max_names);

@@ -77,6 +77,22 @@ class BatchTuning(C.Structure):
                 ("planes_in_flight", C.c_int)]
 
 
+class ServerDesc(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("hbm_budget", C.c_uint64),
+                ("max_batch_jobs", C.c_int), ("streams", C.c_int), ("solo_vis", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch_id", C.c_uint64), ("batch_jobs", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64),
+                ("vis_done", C.c_uint64), ("batches", C.c_uint64), ("bytes_in_use", C.c_uint64),
+                ("peak_bytes", C.c_uint64), ("jobs_waiting", C.c_uint64)]
+
+
 _lib = None
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -132,6 +148,11 @@ def lib():
     L.rick_batch_get_stats.argtypes = [_vp, C.POINTER(PlanStats)]
     L.rick_batch_destroy.argtypes = [_vp]
     L.rick_batch_kernels_per_run.argtypes = [_vp, C.POINTER(C.c_uint32)]
+    L.rick_server_create.argtypes = [C.POINTER(_vp), C.POINTER(ServerDesc)]
+    L.rick_server_submit.argtypes = [_vp, C.POINTER(JobDesc), C.POINTER(C.c_uint64)]
+    L.rick_server_wait.argtypes = [_vp, C.c_uint64, C.c_double, C.POINTER(JobResult)]
+    L.rick_server_get_stats.argtypes = [_vp, C.POINTER(ServerStats)]
+    L.rick_server_destroy.argtypes = [_vp]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
     L.rick_launch_count.argtypes = []
     L.rick_launch_count.restype = C.c_ulonglong
@@ -141,7 +162,9 @@ def lib():
                "rick_kernel_names", "rick_fft_planes", "rick_plan_set_timing",
                "rick_plan_stage_ms", "rick_batch_footprint", "rick_batch_create",
                "rick_batch_run", "rick_batch_get_tuning", "rick_batch_get_stats",
-               "rick_batch_destroy", "rick_batch_kernels_per_run"]:
+               "rick_batch_destroy", "rick_batch_kernels_per_run", "rick_server_create",
+               "rick_server_submit", "rick_server_wait", "rick_server_get_stats",
+               "rick_server_destroy"]:
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L
@@ -427,6 +450,61 @@ class Batch:
         if getattr(self, "_h", None):
             lib().rick_batch_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+# ---- served imaging (continuous batching) ------------------------------------
+
+class Server:
+    """Request loop with continuous batching (include/rick_b200.h, section 5):
+    ``submit`` queues a job and returns a ticket at once; ``wait`` blocks until
+    that job's image is complete and returns its latencies."""
+
+    def __init__(self, precision="mixed", device=0, hbm_budget=150 * 10**9, max_batch_jobs=64,
+                 streams=2, solo_vis=0):
+        d = ServerDesc(device, PRECISIONS[precision], int(hbm_budget), max_batch_jobs, streams,
+                       int(solo_vis))
+        h = _vp()
+        check(lib().rick_server_create(C.byref(h), C.byref(d)), "rick_server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, job: Job) -> int:
+        t = C.c_uint64()
+        d = job.desc()
+        check(lib().rick_server_submit(self._h, C.byref(d), C.byref(t)), "rick_server_submit")
+        self._keep[int(t.value)] = job  # the job's buffers stay alive until waited for
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0) -> dict:
+        r = JobResult()
+        st = lib().rick_server_wait(self._h, ticket, timeout_ms, C.byref(r))
+        self._keep.pop(ticket, None)
+        check(st, "rick_server_wait")
+        return {k: (float(getattr(r, k)) if k.endswith("_ms") else int(getattr(r, k)))
+                for k, _ in JobResult._fields_}
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib().rick_server_get_stats(self._h, C.byref(s)), "rick_server_get_stats")
+        return {k: int(getattr(s, k)) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rick_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
 
     def __del__(self):
         try:

@@ -187,7 +187,9 @@ int batch_launch(rick_batch *b, cudaStream_t st) {
   return RICK_OK;
 }
 
-int build_tables(rick_batch *b) {
+// Device tables of the batch, copied on `st` (from pageable memory: each call
+// returns once its source has been staged).
+int build_tables(rick_batch *b, cudaStream_t st) {
   const int n = (int)b->jobs.size();
   const Layout &L = b->L;
   char *A = b->arena;
@@ -200,7 +202,8 @@ int build_tables(rick_batch *b) {
     std::vector<float2> t32(len);
     make_twiddles(len, t64.data(), t32.data());
     const void *src = f64 ? (const void *)t64.data() : (const void *)t32.data();
-    RICK_CUDA(cudaMemcpy(A + kv.second, src, (size_t)len * (f64 ? 16 : 8), cudaMemcpyHostToDevice));
+    RICK_CUDA(cudaMemcpyAsync(A + kv.second, src, (size_t)len * (f64 ? 16 : 8),
+                              cudaMemcpyHostToDevice, st));
     tw[kv.first] = A + kv.second;
   }
   std::vector<BatchJob> hj(n);
@@ -230,6 +233,13 @@ int build_tables(rick_batch *b) {
     J.nrows = d.num_rows;
     J.nchan = d.freq_per_chan;
     J.npol = d.polarizations;
+    {
+      const uint32_t nv = d.freq_per_chan * d.polarizations;
+      const bool aligned = ((uintptr_t)d.vis_real % 16 == 0) && ((uintptr_t)d.vis_img % 16 == 0);
+      J.scatter_v4 = aligned && nv % 4 == 0 &&
+                     (d.polarizations == 1 || d.polarizations == 2 || d.polarizations == 4);
+      J.scatter_lanes = lanes_per_row(J.scatter_v4 ? nv / 4 : nv);
+    }
     J.bin_base = bb;
     J.counts_base = cb;
     J.mask_base = mb;
@@ -266,9 +276,10 @@ int build_tables(rick_batch *b) {
     lb += (uint64_t)g.nw * g.ny;
     lm.assign(g.nx + g.ny, 0.0);
     phase_tables(g.nx, g.ny, g.nx, g.ny, d.resolution, lm.data(), lm.data() + g.nx);
-    RICK_CUDA(cudaMemcpy(A + L.lm[j], lm.data(), lm.size() * 8, cudaMemcpyHostToDevice));
+    RICK_CUDA(cudaMemcpyAsync(A + L.lm[j], lm.data(), lm.size() * 8, cudaMemcpyHostToDevice, st));
     make_table(d.kernel, d.w_support, tab.data());
-    RICK_CUDA(cudaMemcpy(A + L.table[j], tab.data(), tab.size() * 8, cudaMemcpyHostToDevice));
+    RICK_CUDA(cudaMemcpyAsync(A + L.table[j], tab.data(), tab.size() * 8, cudaMemcpyHostToDevice,
+                              st));
   }
   row_units[n] = ru;
   bin_base[n] = bb;
@@ -276,11 +287,13 @@ int build_tables(rick_batch *b) {
   std::vector<uint32_t> tabs(3 * n + 2, 0);
   FftJobs &f = b->fj;
   fft_classes(hj.data(), n, f, tabs.data() + (n + 1), tabs.data() + (2 * n + 1));
-  RICK_CUDA(cudaMemcpy(A + L.jobs, hj.data(), sizeof(BatchJob) * n, cudaMemcpyHostToDevice));
-  RICK_CUDA(cudaMemcpy(A + L.row_units, row_units.data(), 8 * (n + 1), cudaMemcpyHostToDevice));
-  RICK_CUDA(cudaMemcpy(A + L.bin_base, bin_base.data(), 4 * (n + 1), cudaMemcpyHostToDevice));
-  RICK_CUDA(cudaMemcpy(A + L.mask_base, mask_base.data(), 8 * (n + 1), cudaMemcpyHostToDevice));
-  RICK_CUDA(cudaMemcpy(A + L.fft_tabs, tabs.data(), 4 * tabs.size(), cudaMemcpyHostToDevice));
+  RICK_CUDA(cudaMemcpyAsync(A + L.jobs, hj.data(), sizeof(BatchJob) * n, cudaMemcpyHostToDevice, st));
+  RICK_CUDA(cudaMemcpyAsync(A + L.row_units, row_units.data(), 8 * (n + 1), cudaMemcpyHostToDevice,
+                            st));
+  RICK_CUDA(cudaMemcpyAsync(A + L.bin_base, bin_base.data(), 4 * (n + 1), cudaMemcpyHostToDevice, st));
+  RICK_CUDA(cudaMemcpyAsync(A + L.mask_base, mask_base.data(), 8 * (n + 1), cudaMemcpyHostToDevice,
+                            st));
+  RICK_CUDA(cudaMemcpyAsync(A + L.fft_tabs, tabs.data(), 4 * tabs.size(), cudaMemcpyHostToDevice, st));
 
   BatchLaunch &bl = b->bl;
   bl.jobs = (const BatchJob *)(A + L.jobs);
@@ -289,18 +302,8 @@ int build_tables(rick_batch *b) {
   bl.u.bin_base = (const uint32_t *)(A + L.bin_base);
   bl.total_row_units = L.total_row_units;
   bl.total_bins = L.total_bins;
-  bl.max_nv = 1;
-  bl.v4 = true;
   bl.max_support = 1;
-  for (const rick_job_desc &d : b->jobs) {
-    const uint32_t nv = d.freq_per_chan * d.polarizations;
-    bl.max_nv = std::max<int>(bl.max_nv, (int)nv);
-    bl.max_support = std::max(bl.max_support, d.w_support);
-    const bool aligned = ((uintptr_t)d.vis_real % 16 == 0) && ((uintptr_t)d.vis_img % 16 == 0);
-    if (!(aligned && nv % 4 == 0 && (d.polarizations == 1 || d.polarizations == 2 ||
-                                     d.polarizations == 4)))
-      bl.v4 = false;
-  }
+  for (const rick_job_desc &d : b->jobs) bl.max_support = std::max(bl.max_support, d.w_support);
   bl.rowmask = (uint32_t *)(A + L.rowmask);
   bl.tilemask = (uint32_t *)(A + L.tilemask);
 
@@ -428,8 +431,10 @@ void batch_free(rick_batch *b) {
   delete b;
 }
 
+// st: the stream of the table copies (and of every run: the server's path);
+// nullptr gives the batch its own stream (the graph path).
 int batch_prepare(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
-                  int device, void *arena, uint64_t arena_bytes) {
+                  int device, void *arena, uint64_t arena_bytes, cudaStream_t stream) {
   if (!out) return set_error(RICK_ERR_INVALID_ARG, "null batch pointer");
   *out = nullptr;
   if (njobs <= 0 || !jobs) return set_error(RICK_ERR_INVALID_ARG, "a batch needs at least one job");
@@ -470,11 +475,11 @@ int batch_prepare(rick_batch **out, const rick_job_desc *jobs, int njobs, int pr
       }
     }
   }
-  if (st == RICK_OK) st = build_tables(b);
-  if (st == RICK_OK) {
+  if (st == RICK_OK && !stream) {
     const cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) st = cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
   }
+  if (st == RICK_OK) st = build_tables(b, stream ? stream : b->cap);
   if (st != RICK_OK) {
     batch_free(b);
     return st;
@@ -502,7 +507,7 @@ int rick_batch_footprint(const rick_job_desc *jobs, int njobs, int precision, ui
 
 int rick_batch_create(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
                       int device, const rick_batch_tuning *tuning) {
-  RICK_TRY(batch_prepare(out, jobs, njobs, precision, device, nullptr, 0));
+  RICK_TRY(batch_prepare(out, jobs, njobs, precision, device, nullptr, 0, nullptr));
   rick_batch *b = *out;
   DevGuard guard(b->device);
   int st = RICK_OK;
@@ -515,6 +520,9 @@ int rick_batch_create(rick_batch **out, const rick_job_desc *jobs, int njobs, in
     st = autotune(b);
   }
   if (st == RICK_OK) st = capture(b);
+  // the tables were copied on the batch's own stream; runs go on the caller's
+  if (st == RICK_OK && cudaStreamSynchronize(b->cap) != cudaSuccess)
+    st = cuda_status(cudaGetLastError(), "cudaStreamSynchronize", __FILE__, __LINE__);
   if (st != RICK_OK) {
     batch_free(b);
     *out = nullptr;
@@ -579,8 +587,9 @@ int rick_batch_destroy(rick_batch *b) {
 namespace rick {
 
 int batch_create_in(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
-                    int device, void *arena, uint64_t arena_bytes, const rick_batch_tuning &t) {
-  RICK_TRY(batch_prepare(out, jobs, njobs, precision, device, arena, arena_bytes));
+                    int device, void *arena, uint64_t arena_bytes, const rick_batch_tuning &t,
+                    cudaStream_t st) {
+  RICK_TRY(batch_prepare(out, jobs, njobs, precision, device, arena, arena_bytes, st));
   (*out)->tune = t;
   (*out)->use_graph = false;
   return RICK_OK;
@@ -594,6 +603,16 @@ uint64_t batch_bytes(const rick_job_desc *jobs, int njobs, int precision) {
   uint64_t bytes = 0;
   if (rick_batch_footprint(jobs, njobs, precision, &bytes) != RICK_OK) return 0;
   return bytes;
+}
+
+bool batch_cached_tuning(int precision, rick_batch_tuning *t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto &kv : g_tune_cache)
+    if (kv.first.precision == precision) {
+      *t = kv.second;
+      return true;
+    }
+  return false;
 }
 
 }  // namespace rick

@@ -286,7 +286,8 @@ __global__ void __launch_bounds__(256)
   add_scatter_counts(gridded, nrec, counters);
 }
 
-template <int G, bool V4>
+// The same over every job of a batch; each job has its own lanes per row and
+// load width (warp-uniform: a unit is 32 rows of one job).
 __global__ void __launch_bounds__(256)
     k_bin_scatter_batch(const BatchJob *__restrict__ jobs, int njobs,
                         const uint64_t *__restrict__ row_units, uint64_t total_units,
@@ -299,9 +300,30 @@ __global__ void __launch_bounds__(256)
     const int j = batch_job_of(row_units, njobs, u);
     const BatchJob &J = jobs[j];
     const Geometry g = J.g;
-    scatter_rows<G, V4>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan,
-                        J.npol, g, (u - row_units[j]) * 32, J.bin_base, bin_off, bin_cursor, rec,
-                        gridded, nrec);
+    const uint64_t base = (u - row_units[j]) * 32;
+#define RICK_SC(GG, VV)                                                                          \
+  scatter_rows<GG, VV>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan, J.npol, \
+                       g, base, J.bin_base, bin_off, bin_cursor, rec, gridded, nrec)
+    if (J.scatter_v4) {
+      switch (J.scatter_lanes) {
+        case 1: RICK_SC(1, true); break;
+        case 2: RICK_SC(2, true); break;
+        case 4: RICK_SC(4, true); break;
+        case 8: RICK_SC(8, true); break;
+        case 16: RICK_SC(16, true); break;
+        default: RICK_SC(32, true); break;
+      }
+    } else {
+      switch (J.scatter_lanes) {
+        case 1: RICK_SC(1, false); break;
+        case 2: RICK_SC(2, false); break;
+        case 4: RICK_SC(4, false); break;
+        case 8: RICK_SC(8, false); break;
+        case 16: RICK_SC(16, false); break;
+        default: RICK_SC(32, false); break;
+      }
+    }
+#undef RICK_SC
   }
   add_scatter_counts(gridded, nrec, counters);
 }
@@ -407,29 +429,10 @@ int bin_rows_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cudaStr
   k_item_count<<<blocks_items, 256, 0, st>>>(s.bin_count, nbins, max_chunk, s.item_off);
   RICK_CUDA(cudaGetLastError());
   RICK_TRY(exclusive_scan_u32(s.item_off, s.item_off, nbins + 1, s.scan_tmp, st));
-  const int G = lanes_per_row(b.v4 ? (uint64_t)b.max_nv / 4 : (uint64_t)b.max_nv);
   const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((units + 7) / 8, (uint64_t)sms * 8));
-#define RICK_SCATTER_B(GG)                                                                   \
-  case GG:                                                                                   \
-    RICK_LAUNCHED();                                                                         \
-    if (b.v4)                                                                                \
-      k_bin_scatter_batch<GG, true><<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units,   \
-                                                            units, s.bin_count, s.bin_cursor, \
-                                                            s.records, s.counters);           \
-    else                                                                                     \
-      k_bin_scatter_batch<GG, false><<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units,  \
-                                                             units, s.bin_count, s.bin_cursor, \
-                                                             s.records, s.counters);          \
-    break;
-  switch (G) {
-    RICK_SCATTER_B(1)
-    RICK_SCATTER_B(2)
-    RICK_SCATTER_B(4)
-    RICK_SCATTER_B(8)
-    RICK_SCATTER_B(16)
-    RICK_SCATTER_B(32)
-  }
-#undef RICK_SCATTER_B
+  RICK_LAUNCHED();
+  k_bin_scatter_batch<<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units, units, s.bin_count,
+                                              s.bin_cursor, s.records, s.counters);
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }

@@ -103,6 +103,8 @@ struct BatchJob {
   int logx, logy;                  // log2 of the axes (sparse FFT sizes)
   uint64_t nrows;                  // rows of the job
   uint32_t nchan, npol;
+  int scatter_lanes;               // lanes per row of the sample pass (1, 2, 4, ..., 32)
+  int scatter_v4;                  // 16-byte sample loads (aligned rows, nchan*npol % 4 == 0)
   uint32_t bin_base;               // first global bin (nw*nty*ntx bins per job)
   uint32_t counts_base;            // first word of the job's [1 + nw] row counts
   uint64_t mask_base;              // first word of the job's row mask [nw * nty]
@@ -218,8 +220,6 @@ struct BatchLaunch {
   BatchUnits u;
   uint64_t total_row_units;
   uint32_t total_bins;
-  int max_nv;              // largest nchan*npol
-  bool v4;                 // every job allows 16-byte sample loads
   int max_support;
   uint32_t *rowmask, *tilemask;  // batch-wide arrays
   int grid_blocks_per_sm;  // gridder occupancy (tuned)
@@ -236,6 +236,18 @@ void fft_classes(const BatchJob *host_jobs, int njobs, FftJobs &f, uint32_t *col
 int sparse_fft_lists(const FftJobs &f, cudaStream_t st);  // row lists and row-pass units
 int sparse_fft_rows(const FftJobs &f, int precision, cudaStream_t st);
 int sparse_fft_cols(const FftJobs &f, int precision, cudaStream_t st);
+
+// The batch internals the serving loop (serve.cu) builds on (batch.cu).
+int batch_create_in(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
+                    int device, void *arena, uint64_t arena_bytes, const rick_batch_tuning &t,
+                    cudaStream_t st);
+int batch_launch_eager(rick_batch *b, cudaStream_t st);
+void batch_destroy(rick_batch *b);
+uint64_t batch_bytes(const rick_job_desc *jobs, int njobs, int precision);
+bool batch_cached_tuning(int precision, rick_batch_tuning *t);
+
+// Lanes per row of the sample pass for rows of `per_row` loads (bin.cu).
+int lanes_per_row(uint64_t per_row);
 
 int num_sms();
 
