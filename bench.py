@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-snapshot leg (256 small jobs, one graph)")
     ap.add_argument("--jobs", type=int, default=256, help="jobs of the batched-snapshot leg")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "shard"],
+                    help="N>1: independent jobs per GPU (weak scaling) or one job with its "
+                         "w-planes split over the GPUs and the image all-reduced (strong)")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
     ap.add_argument("--served-requests", type=int, default=300)
     ap.add_argument("--served-rates", type=float, nargs="+", default=[250.0, 500.0, 1000.0, 0.0],
@@ -206,12 +209,20 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
+    shard_mode = world > 1 and args.mode == "shard"
+
     def run_form(precision):
         geom = R.Geometry(nx, ny, nw, cfg.w_support, cfg.kernel, precision)
-        plan = R.Plan(geom, n, nchan, npol, device=local)
         img = torch.empty(2 * nx * ny, dtype=torch.float64, device=dev)
-        step = lambda: plan.image(n, rows, res, wmin, wmax, img[: nx * ny], img[nx * ny:],
-                                  R.ROWS_SECTOR0, stream)
+        if shard_mode:
+            from rick_b200.shard import ShardedImager
+            imager = ShardedImager(geom, n, nchan, npol, device=local)
+            plan = imager.plan
+            step = lambda: imager.image(n, rows, res, wmin, wmax, img, R.ROWS_SECTOR0, stream)
+        else:
+            plan = R.Plan(geom, n, nchan, npol, device=local)
+            step = lambda: plan.image(n, rows, res, wmin, wmax, img[: nx * ny], img[nx * ny:],
+                                      R.ROWS_SECTOR0, stream)
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
@@ -230,21 +241,24 @@ def run_ours(args):
         ms = e0.elapsed_time(e1) / args.steps
         barrier()
         # per-stage times (stage events on the same stream), a second pass
-        plan.set_timing(True)
-        stage = {}
-        lat = []
-        for _ in range(max(3, min(args.steps, 10))):
-            step()
-            s = plan.stage_ms()
-            lat.append(sum(s.values()))
-            for k, v in s.items():
-                stage[k] = stage.get(k, 0.0) + v
+        stage, lat = {}, []
         k = max(3, min(args.steps, 10))
-        stage = {kk: v / k for kk, v in stage.items()}
-        plan.set_timing(False)
-        stats = plan.stats()
+        if plan is not None:
+            plan.set_timing(True)
+        for _ in range(k):
+            step()
+            s = plan.stage_ms() if plan is not None else {}
+            lat.append(sum(s.values()))
+            for kk, v in s.items():
+                stage[kk] = stage.get(kk, 0.0) + v
+        stage = {kk: v / k for kk, v in stage.items()} or {"phase": 0.0}
+        stats = plan.stats() if plan is not None else {"records": 0, "rows_gridded": 0,
+                                                       "rows_dropped": 0, "work_items": 0}
+        if plan is not None:
+            plan.set_timing(False)
         image = img.clone()
-        return plan, image, ms, stage, stats, launches, lat
+        closer = imager if shard_mode else plan
+        return closer, image, ms, stage, stats, launches, lat
 
     forms = args.forms.split(",")
     with ClockSampler(local) as clocks:
@@ -262,11 +276,12 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms64, msmx = float(t[0]), float(t[1])
-    value = world * nvis / (ms64 * 1e-3)
+    jobs_done = 1 if shard_mode else world   # one job split over the GPUs, or one per GPU
+    value = jobs_done * nvis / (ms64 * 1e-3)
 
     # ---- e2e through the host C-ABI entry point (pinned host buffers)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not shard_mode:  # shard mode: device-resident rows only
         host = [r.cpu().pin_memory() for r in rows]
         h_img = torch.empty(2 * nx * ny, dtype=torch.float64).pin_memory()
         geom = R.Geometry(nx, ny, nw, cfg.w_support, cfg.kernel, "fp64")
@@ -316,24 +331,27 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "strong" if shard_mode else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "config": {"workload": "LOFAR-like single image: 5,096,600 rows x 64 chan x 4 pol "
                                "(1.305e9 vis), 4096^2 x 32 w-planes, Kaiser-Bessel support 7",
                    "rows": n, "visibilities": nvis, "grid": nx, "w_planes": nw,
                    "kernel": cfg.kernel, "w_support": cfg.w_support,
                    "l2": f"inputs ({in_bytes / 1e9:.2f} GB) larger than L2; no flush"
                          if in_bytes > 126e6 else "inputs smaller than L2",
-                   "parallelism": f"replicas x{world}", "time_fraction": args.time_fraction},
+                   "parallelism": (f"w-plane shards x{world} + NCCL image all-reduce" if shard_mode
+                                   else f"replicas x{world}"),
+                   "time_fraction": args.time_fraction},
         "e2e": e2e, "gpu_launches": launches,
         "roofline": roofline,
         "pipeline_roofline": {"bytes": pipe_bytes, "achieved_gbs": pipe_bytes / (ms64 * 1e-3) / 1e9,
                               "frac": pipe_bytes / (ms64 * 1e-3) / 1e9 / hbm},
-        "forms": {"fp64": {"vis_per_s": world * nvis / (ms64 * 1e-3), "ms": ms64,
+        "forms": {"fp64": {"vis_per_s": jobs_done * nvis / (ms64 * 1e-3), "ms": ms64,
                            "stages_ms": stage64,
                            "p50_ms": float(np.percentile(lat64, 50)),
                            "p99_ms": float(np.percentile(lat64, 99))},
                   "mixed": None if "mixed" not in forms else {
-                      "vis_per_s": world * nvis / (msmx * 1e-3), "ms": msmx,
+                      "vis_per_s": jobs_done * nvis / (msmx * 1e-3), "ms": msmx,
                       "stages_ms": stagemx,
                       "p50_ms": float(np.percentile(latmx, 50)),
                       "p99_ms": float(np.percentile(latmx, 99)),

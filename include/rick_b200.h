@@ -113,6 +113,13 @@ typedef struct rick_plan_desc {
   uint64_t max_rows;      /* capacity: rows per call */
   uint32_t freq_per_chan; /* channels per row */
   uint32_t polarizations; /* polarisations per row (1, 2 or 4 vectorise) */
+  /* w-plane shard: the plan holds planes w_first .. w_first+w_count-1 of the
+   * num_w_planes-plane cube (0, 0: all).  Rows are assigned to planes with the
+   * whole cube's dw; rows of other planes are skipped (rows_other_shard); the
+   * image is this shard's part of the plane sum (the w-correction uses the
+   * global plane index), so the shards' images add up to the whole image. */
+  int w_first;
+  int w_count;
 } rick_plan_desc;
 
 typedef struct rick_plan_stats {
@@ -124,6 +131,7 @@ typedef struct rick_plan_stats {
   uint64_t device_bytes;   /* HBM held by the plan */
   uint64_t fft_rows;       /* (plane, row) pairs the last rick_plan_image transformed on its
                               sparse path (rows the gridder touched); 0 after the dense path */
+  uint64_t rows_other_shard; /* rows of planes outside the plan's w-plane shard */
 } rick_plan_stats;
 
 /* Row selection applied by the gridding calls. */

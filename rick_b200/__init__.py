@@ -51,14 +51,15 @@ class PlanDesc(C.Structure):
     _fields_ = [("grid_size_x", C.c_int), ("grid_size_y", C.c_int), ("num_w_planes", C.c_int),
                 ("w_support", C.c_int), ("kernel", C.c_int), ("precision", C.c_int),
                 ("phase_on", C.c_int), ("device", C.c_int), ("max_rows", C.c_uint64),
-                ("freq_per_chan", C.c_uint32), ("polarizations", C.c_uint32)]
+                ("freq_per_chan", C.c_uint32), ("polarizations", C.c_uint32),
+                ("w_first", C.c_int), ("w_count", C.c_int)]
 
 
 class PlanStats(C.Structure):
     _fields_ = [("rows_in", C.c_uint64), ("rows_gridded", C.c_uint64),
                 ("rows_dropped", C.c_uint64), ("records", C.c_uint64),
                 ("work_items", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("fft_rows", C.c_uint64)]
+                ("fft_rows", C.c_uint64), ("rows_other_shard", C.c_uint64)]
 
 
 class JobDesc(C.Structure):
@@ -281,11 +282,14 @@ class Plan:
     """Device-resident imaging plan (rick_plan_* in include/rick_b200.h)."""
 
     def __init__(self, geom: Geometry, max_rows: int, freq_per_chan: int, polarizations: int,
-                 device: int = -1):
+                 device: int = -1, planes: Optional[tuple] = None):
+        """``planes=(w_first, w_count)`` makes the plan one w-plane shard of the cube."""
         self.geom = geom
+        w_first, w_count = planes if planes is not None else (0, 0)
         self.desc = PlanDesc(geom.grid_size_x, geom.grid_size_y, geom.num_w_planes,
                              geom.w_support, KERNELS[geom.kernel], PRECISIONS[geom.precision],
-                             int(geom.phase_on), device, max_rows, freq_per_chan, polarizations)
+                             int(geom.phase_on), device, max_rows, freq_per_chan, polarizations,
+                             w_first, w_count)
         h = _vp()
         check(lib().rick_plan_create(C.byref(h), C.byref(self.desc)), "rick_plan_create")
         self._h = h

@@ -27,8 +27,9 @@ constexpr uint32_t kNoBin = 0xffffffffu;
 
 struct RowPos {
   double pu, pv;  // pos_u, pos_v
-  int gu, gv, gw;
-  bool keep;
+  int gu, gv, gw;  // gw: plane within the shard
+  bool keep;       // gridded here
+  bool other;      // a valid row of a plane outside the shard
 };
 
 // gridding.c:149-188 with nsectors = 1 and yaxis = grid_size_y: the rows one
@@ -45,7 +46,8 @@ __device__ __forceinline__ bool in_sector0(double v, const Geometry &g) {
 
 // w-stacking.cu:143-149.  Rows whose plane index falls outside the cube, or
 // whose footprint bounds would wrap as unsigned in the reference
-// (grid_u < -KernelLen), are dropped and counted.
+// (grid_u < -KernelLen), are dropped and counted.  With a w-plane shard, valid
+// rows of the other shards' planes are skipped (counted apart).
 __device__ __forceinline__ RowPos row_position(double u, double v, double w, const Geometry &g) {
   RowPos p;
   p.pu = __ddiv_rn(u, g.dx);
@@ -54,9 +56,12 @@ __device__ __forceinline__ RowPos row_position(double u, double v, double w, con
   p.gw = (int)wi;
   p.gu = (int)p.pu;
   p.gv = (int)p.pv;
-  bool keep = p.gw >= 0 && p.gw < g.nw && p.gu >= -g.half && p.gv >= -g.half;
+  const int ntot = g.nw_total > 0 ? g.nw_total : g.nw;
+  bool keep = p.gw >= 0 && p.gw < ntot && p.gu >= -g.half && p.gv >= -g.half;
   if (g.select_sector0) keep = keep && in_sector0(v, g);
-  p.keep = keep;
+  p.other = keep && (p.gw < g.w_first || p.gw >= g.w_first + g.nw);
+  p.keep = keep && !p.other;
+  p.gw -= g.w_first;
   return p;
 }
 
@@ -85,12 +90,14 @@ __device__ __forceinline__ void offset_bins(uint32_t bins[4], uint32_t bin_base)
 
 // Pass 1 over rows base..base+31 (one per lane): histogram of records per bin.
 // Lanes of a warp that hit the same bin combine their increments (the uv
-// centre is dense).  Returns 1 on a lane whose row was dropped.
+// centre is dense).  Returns 1 on a lane whose row was dropped; `other` counts
+// rows of other shards.
 __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
                                                const double *__restrict__ vv,
                                                const double *__restrict__ ww, uint64_t nrows,
                                                const Geometry &g, uint64_t base,
-                                               uint32_t bin_base, uint32_t *__restrict__ bin_count) {
+                                               uint32_t bin_base, uint32_t *__restrict__ bin_count,
+                                               uint32_t &other) {
   const unsigned lane = lane_id();
   const uint64_t i = base + lane;
   RowPos p;
@@ -98,7 +105,8 @@ __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
   uint32_t dropped = 0;
   if (i < nrows) {
     p = row_position(uu[i], vv[i], ww[i], g);
-    dropped = p.keep ? 0u : 1u;
+    dropped = (p.keep || p.other) ? 0u : 1u;
+    other += p.other ? 1u : 0u;
   }
   uint32_t bins[4];
   footprint_bins(p, g, bins);
@@ -112,9 +120,13 @@ __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
   return dropped;
 }
 
-__device__ __forceinline__ void add_dropped(uint32_t dropped, uint64_t *counters) {
-  for (int o = 16; o; o >>= 1) dropped += __shfl_xor_sync(kFull, dropped, o);
+__device__ __forceinline__ void add_dropped(uint32_t dropped, uint32_t other, uint64_t *counters) {
+  for (int o = 16; o; o >>= 1) {
+    dropped += __shfl_xor_sync(kFull, dropped, o);
+    other += __shfl_xor_sync(kFull, other, o);
+  }
   if (lane_id() == 0 && dropped) atomicAdd((unsigned long long *)&counters[kCntDropped], dropped);
+  if (lane_id() == 0 && other) atomicAdd((unsigned long long *)&counters[kCntOtherShard], other);
 }
 
 __global__ void k_bin_count(const double *__restrict__ uu, const double *__restrict__ vv,
@@ -122,10 +134,10 @@ __global__ void k_bin_count(const double *__restrict__ uu, const double *__restr
                             uint32_t *__restrict__ bin_count, uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
-  uint32_t dropped = 0;
+  uint32_t dropped = 0, other = 0;
   for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32)
-    dropped += count_rows(uu, vv, ww, nrows, g, base, 0, bin_count);
-  add_dropped(dropped, counters);
+    dropped += count_rows(uu, vv, ww, nrows, g, base, 0, bin_count, other);
+  add_dropped(dropped, other, counters);
 }
 
 // The same over every job of a batch: one warp per 32-row unit of one job.
@@ -135,15 +147,15 @@ __global__ void k_bin_count_batch(const BatchJob *__restrict__ jobs, int njobs,
                                   uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
-  uint32_t dropped = 0;
+  uint32_t dropped = 0, other = 0;
   for (uint64_t u = warp; u < total_units; u += nwarps) {
     const int j = batch_job_of(row_units, njobs, u);
     const BatchJob &J = jobs[j];
     const Geometry g = J.g;
     dropped += count_rows(J.uu, J.vv, J.ww, J.nrows, g, (u - row_units[j]) * 32, J.bin_base,
-                          bin_count);
+                          bin_count, other);
   }
-  add_dropped(dropped, counters);
+  add_dropped(dropped, other, counters);
 }
 
 // Work items of the gridder: a bin with c records is split into ceil(c/max_chunk)

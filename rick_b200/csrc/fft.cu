@@ -515,6 +515,7 @@ constexpr int kAnchor = 8;
 template <typename T> struct ColJob {
   const typename V2<T>::t *cube;  // column-blocked row transforms
   int nx, ny, nw, nty;
+  int w_first, nw_total;          // w-plane shard: global index of local plane 0, cube planes
   const uint32_t *rowmask;        // [nw * nty]
   const uint32_t *counts;         // [1 + nw]
   const typename V2<T>::t *tw;    // twiddles of the y axis
@@ -551,7 +552,7 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   double2 *sstep = tables + grp * N;  // RECUR only
   // row masks of the planes of the next two sets (2 * PP slots)
   uint32_t *smask = reinterpret_cast<uint32_t *>(tables + (RECUR ? rpc * N : 0));
-  const bool phase = J.phase_on && nw > 1;
+  const bool phase = J.phase_on && J.nw_total > 1;
   const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
   auto next_plane = [&](int iw) {
     do { iw++; } while (iw < nw && counts[1 + iw] == 0);  // planes without data add exact zeros
@@ -656,7 +657,7 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
       double cw = 0.0;
       if (anchor) {
         last_anchor = iw;
-        cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)iw, J.dw)));  // 2 pi wterm
+        cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + iw), J.dw)));  // 2 pi wterm
       }
       prev_iw = iw;
 #pragma unroll
@@ -748,6 +749,8 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
     J.ny = B.g.ny;
     J.nw = B.g.nw;
     J.nty = B.g.nty;
+    J.w_first = B.g.w_first;
+    J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
     J.rowmask = rowmask + B.mask_base;
     J.counts = counts + B.counts_base;
     J.tw = (const V *)B.tw_y;
@@ -824,6 +827,8 @@ template <typename T> ColJob<T> col_job(const BatchJob &B, const FftJobs &f) {
   J.ny = B.g.ny;
   J.nw = B.g.nw;
   J.nty = B.g.nty;
+  J.w_first = B.g.w_first;
+  J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
   J.rowmask = f.rowmask + B.mask_base;
   J.counts = f.counts + B.counts_base;
   J.tw = (const V *)B.tw_y;

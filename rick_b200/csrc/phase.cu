@@ -25,6 +25,7 @@ template <> struct Vec2<float> { using type = float2; };
 template <typename InT>
 __global__ void __launch_bounds__(256)
     k_phase_sum(const typename Vec2<InT>::type *__restrict__ cube, int xaxis, int yaxis, int nw,
+                int w_first, int nw_total,
                 const double *__restrict__ ltab, const double *__restrict__ mtab, double wmin,
                 double dw, double dwnorm, double norm, int phase_on, int accumulate,
                 double *__restrict__ img_re, double *__restrict__ img_im) {
@@ -35,7 +36,7 @@ __global__ void __launch_bounds__(256)
   const int iu = (int)(pix % xaxis);
   double acc_re = accumulate ? img_re[pix] : 0.0;
   double acc_im = accumulate ? img_im[pix] : 0.0;
-  if (phase_on && nw > 1) {
+  if (phase_on && nw_total > 1) {
     const double l = ltab[iu], m = mtab[iv];
     const double radius2 = __dadd_rn(__dmul_rn(l, l), __dmul_rn(m, m));
     const double root = __dsqrt_rn(__dsub_rn(1.0, radius2));
@@ -43,7 +44,7 @@ __global__ void __launch_bounds__(256)
     const double twopi = 2.0 * kPi;  // exact doubling
 #pragma unroll 4
     for (int iw = 0; iw < nw; iw++) {
-      const double wterm = __dadd_rn(wmin, __dmul_rn((double)iw, dw));
+      const double wterm = __dadd_rn(wmin, __dmul_rn((double)(w_first + iw), dw));
       const double arg = __dmul_rn(__dmul_rn(twopi, wterm), rootm1);
       double s, c;
       sincos(arg, &s, &c);
@@ -81,21 +82,24 @@ void phase_tables(int xaxis, int yaxis, int xaxistot, int yaxistot, double resol
   }
 }
 
-int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, const double *ltab,
-              const double *mtab, double wmin, double wmax, double norm, int phase_on,
-              int accumulate, double *img_re, double *img_im, cudaStream_t st) {
-  // phase_correction.cu:100-102
-  const double dw = (wmax - wmin) / (double)nw;
+int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, int w_first,
+              int nw_total, const double *ltab, const double *mtab, double wmin, double wmax,
+              double norm, int phase_on, int accumulate, double *img_re, double *img_im,
+              cudaStream_t st) {
+  // phase_correction.cu:100-102 (the whole cube's plane spacing)
+  const double dw = (wmax - wmin) / (double)nw_total;
   const double dwnorm = dw / (wmax - wmin);
   const uint64_t plane = (uint64_t)xaxis * yaxis;
   if (plane == 0) return RICK_OK;
   const unsigned blocks = (unsigned)((plane + 255) / 256);
   if (precision == RICK_PREC_FP64)
-    k_phase_sum<double><<<blocks, 256, 0, st>>>((const double2 *)cube, xaxis, yaxis, nw, ltab,
+    k_phase_sum<double><<<blocks, 256, 0, st>>>((const double2 *)cube, xaxis, yaxis, nw, w_first,
+                                                nw_total, ltab,
                                                 mtab, wmin, dw, dwnorm, norm, phase_on,
                                                 accumulate, img_re, img_im);
   else
-    k_phase_sum<float><<<blocks, 256, 0, st>>>((const float2 *)cube, xaxis, yaxis, nw, ltab, mtab,
+    k_phase_sum<float><<<blocks, 256, 0, st>>>((const float2 *)cube, xaxis, yaxis, nw, w_first,
+                                               nw_total, ltab, mtab,
                                                wmin, dw, dwnorm, norm, phase_on, accumulate,
                                                img_re, img_im);
   RICK_CUDA(cudaGetLastError());

@@ -173,6 +173,9 @@ int dev_alloc(rick_plan *p, void **ptr, size_t bytes) {
   return RICK_OK;
 }
 
+// Planes the plan holds: its w-plane shard, or the whole cube.
+int plan_planes(const rick_plan_desc *d) { return d->w_count > 0 ? d->w_count : d->num_w_planes; }
+
 int validate_desc(const rick_plan_desc *d) {
   if (!d) return set_error(RICK_ERR_INVALID_ARG, "null plan description");
   if (d->grid_size_x <= 0 || d->grid_size_y <= 0 || d->num_w_planes <= 0)
@@ -187,7 +190,12 @@ int validate_desc(const rick_plan_desc *d) {
     return set_error(RICK_ERR_INVALID_ARG, "unknown precision %d", d->precision);
   if (d->freq_per_chan == 0 || d->polarizations == 0)
     return set_error(RICK_ERR_INVALID_ARG, "freq_per_chan and polarizations must be positive");
-  const uint64_t nbins = (uint64_t)d->num_w_planes * ((d->grid_size_x + kTile - 1) / kTile) *
+  if (d->w_count < 0 || d->w_first < 0 ||
+      (d->w_count > 0 && d->w_first + d->w_count > d->num_w_planes) ||
+      (d->w_count == 0 && d->w_first != 0))
+    return set_error(RICK_ERR_INVALID_ARG, "w-plane shard %d+%d outside the %d planes", d->w_first,
+                     d->w_count, d->num_w_planes);
+  const uint64_t nbins = (uint64_t)plan_planes(d) * ((d->grid_size_x + kTile - 1) / kTile) *
                          ((d->grid_size_y + kTile - 1) / kTile);
   if (nbins >= 0xffffffffull) return set_error(RICK_ERR_INVALID_ARG, "grid too large");
   if (4 * d->max_rows >= 0xffffffffull)
@@ -199,7 +207,9 @@ void fill_geometry(rick_plan *p, double dx, double dw, int select) {
   Geometry &g = p->g;
   g.nx = p->d.grid_size_x;
   g.ny = p->d.grid_size_y;
-  g.nw = p->d.num_w_planes;
+  g.nw = plan_planes(&p->d);
+  g.w_first = p->d.w_count > 0 ? p->d.w_first : 0;
+  g.nw_total = p->d.num_w_planes;
   g.support = p->d.w_support;
   g.half = (p->d.w_support - 1) / 2;
   g.ntx = (g.nx + kTile - 1) / kTile;
@@ -215,7 +225,7 @@ struct FftBytes {
 };
 
 int choose_fft(rick_plan *p) {
-  const int nx = p->d.grid_size_x, ny = p->d.grid_size_y, nw = p->d.num_w_planes;
+  const int nx = p->d.grid_size_x, ny = p->d.grid_size_y, nw = plan_planes(&p->d);
   int n[2] = {ny, nx};
   const cufftType type = p->d.precision == RICK_PREC_FP64 ? CUFFT_Z2Z : CUFFT_C2C;
   const long long plane = (long long)nx * ny;
@@ -384,7 +394,7 @@ int plan_fft_impl(rick_plan *p, cudaStream_t st) {
   RICK_CUFFT(cufftSetStream(p->fft, st));
   RICK_TRY(mark(p, p->ev_fft0, st));
   const uint64_t plane = (uint64_t)p->d.grid_size_x * p->d.grid_size_y;
-  for (int b0 = 0; b0 < p->d.num_w_planes; b0 += p->fft_batch) {
+  for (int b0 = 0; b0 < plan_planes(&p->d); b0 += p->fft_batch) {
     if (p->d.precision == RICK_PREC_FP64) {
       cufftDoubleComplex *ptr = (cufftDoubleComplex *)p->cube + (uint64_t)b0 * plane;
       RICK_CUFFT(cufftExecZ2Z(p->fft, ptr, ptr, CUFFT_INVERSE));
@@ -414,7 +424,8 @@ int plan_phase_impl(rick_plan *p, int xtot, int ytot, double resolution, double 
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
   RICK_TRY(ensure_lm(p, nx, ny, xtot, ytot, resolution, st));
   RICK_TRY(mark(p, p->ev_phase0, st));
-  RICK_TRY(phase_sum(p->d.precision, p->cube, nx, ny, p->d.num_w_planes, p->d_lm, p->d_lm + nx,
+  RICK_TRY(phase_sum(p->d.precision, p->cube, nx, ny, plan_planes(&p->d), p->g.w_first,
+                     p->d.num_w_planes, p->d_lm, p->d_lm + nx,
                      wmin, wmax, cube_scale(p), p->d.phase_on, accumulate, img_re, img_im, st));
   g_launches++;
   RICK_TRY(mark(p, p->ev[6], st));
@@ -428,7 +439,7 @@ extern "C" {
 
 int rick_plan_footprint(const rick_plan_desc *desc, uint64_t *bytes) {
   RICK_TRY(validate_desc(desc));
-  const uint64_t nx = desc->grid_size_x, ny = desc->grid_size_y, nw = desc->num_w_planes;
+  const uint64_t nx = desc->grid_size_x, ny = desc->grid_size_y, nw = plan_planes(desc);
   const uint64_t nbins = nw * ((nx + kTile - 1) / kTile) * ((ny + kTile - 1) / kTile);
   const uint64_t vb = desc->precision == RICK_PREC_FP64 ? 8 : 4;
   uint64_t b = 2 * nw * nx * ny * vb;                      // cube
@@ -460,7 +471,8 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
   fill_geometry(p, 1.0 / desc->grid_size_x, 1.0 / desc->num_w_planes, 0);
   const uint64_t nbins = p->g.nbins();
   p->val_bytes = desc->precision == RICK_PREC_FP64 ? 8 : 4;
-  p->cube_vals = 2ull * desc->num_w_planes * desc->grid_size_x * desc->grid_size_y;
+  const int nwl = plan_planes(desc);
+  p->cube_vals = 2ull * nwl * desc->grid_size_x * desc->grid_size_y;
   int st = RICK_OK;
   auto A = [&](void **ptr, size_t bytes) {
     if (st == RICK_OK) st = dev_alloc(p, ptr, bytes);
@@ -490,10 +502,10 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
               getenv("RICK_DENSE_FFT") == nullptr;
   if (st == RICK_OK && p->sparse) {
     const int nx = desc->grid_size_x, ny = desc->grid_size_y;
-    A((void **)&p->f.rowmask, (size_t)desc->num_w_planes * p->g.nty * 4);
-    A((void **)&p->f.rowlist, (size_t)desc->num_w_planes * ny * 4);
-    A((void **)&p->f.counts, (size_t)(1 + desc->num_w_planes) * 4);
-    A((void **)&p->f.tilemask, (size_t)desc->num_w_planes * p->g.nty * ((p->g.ntx + 31) / 32) * 4);
+    A((void **)&p->f.rowmask, (size_t)nwl * p->g.nty * 4);
+    A((void **)&p->f.rowlist, (size_t)nwl * ny * 4);
+    A((void **)&p->f.counts, (size_t)(1 + nwl) * 4);
+    A((void **)&p->f.tilemask, (size_t)nwl * p->g.nty * ((p->g.ntx + 31) / 32) * 4);
     A((void **)&p->f.tw_x64, (size_t)nx * sizeof(double2));
     A((void **)&p->f.tw_y64, (size_t)ny * sizeof(double2));
     A((void **)&p->f.tw_x32, (size_t)nx * sizeof(float2));
@@ -525,7 +537,7 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
       BatchJob hj = plan_job(p);
       uint32_t tabs[8] = {};
       fft_classes(&hj, 1, fj, tabs + 2, tabs + 3);
-      const uint64_t mb[2] = {0, (uint64_t)desc->num_w_planes * p->g.nty};
+      const uint64_t mb[2] = {0, (uint64_t)nwl * p->g.nty};
       fj.jobs = p->d_job;
       fj.njobs = 1;
       fj.fft_units = p->d_fft_tabs;
@@ -533,7 +545,7 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
       fj.col_units = p->d_fft_tabs + 3;
       fj.mask_base = p->d_mask_base;
       fj.total_mask_words = mb[1];
-      fj.total_count_words = 1 + desc->num_w_planes;
+      fj.total_count_words = 1 + nwl;
       fj.rowmask = p->f.rowmask;
       fj.tilemask = p->f.tilemask;
       fj.rowlist = p->f.rowlist;
@@ -773,6 +785,7 @@ int rick_plan_get_stats(rick_plan *p, rick_plan_stats *out) {
   RICK_CUDA(cudaMemcpy(&items, p->s.item_off + p->g.nbins(), 4, cudaMemcpyDeviceToHost));
   out->work_items = items;
   out->device_bytes = p->device_bytes;
+  out->rows_other_shard = c[kCntOtherShard];
   if (p->cube_state == kCubeSparse) {
     uint32_t rows = 0;
     RICK_CUDA(cudaMemcpy(&rows, p->f.counts, 4, cudaMemcpyDeviceToHost));

@@ -56,6 +56,8 @@ struct Geometry {
   double dx, dw;        // 1/Nx, 1/Nw (init.c:11-12) or as passed to wstack
   double w_supporth;    // (double)half*dx (init.c:13)
   int select_sector0;   // apply gridding.c:149-188 membership
+  int w_first;          // first plane of a w-plane shard (nw planes from here)
+  int nw_total;         // planes of the whole cube (0: nw)
   uint64_t nbins() const { return (uint64_t)nw * ntx * nty; }
 };
 
@@ -169,6 +171,7 @@ enum Counter : int {
   kCntItemNext = 3,   // persistent gridder work counter
   kCntHeavy = 4,      // number of heavy bins
   kCntOverflow = 5,   // records beyond capacity (must stay 0)
+  kCntOtherShard = 6, // rows of planes outside the shard
   kNumCounters = 8
 };
 
@@ -191,9 +194,12 @@ bool sparse_fft_supported(int nx, int ny);
 void make_twiddles(int n, double2 *t64, float2 *t32);
 void phase_tables(int xaxis, int yaxis, int xaxistot, int yaxistot, double resolution,
                   double *l, double *m);
-int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, const double *ltab,
-              const double *mtab, double wmin, double wmax, double norm, int phase_on,
-              int accumulate, double *img_re, double *img_im, cudaStream_t st);
+// Planes w_first .. w_first+nw-1 of an nw_total-plane cube (phase_correction
+// with the global plane index; nw_total = nw, w_first = 0 for a whole cube).
+int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, int w_first,
+              int nw_total, const double *ltab, const double *mtab, double wmin, double wmax,
+              double norm, int phase_on, int accumulate, double *img_re, double *img_im,
+              cudaStream_t st);
 int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *tmp,
                        cudaStream_t st);
 uint64_t scan_tmp_words(uint64_t n);
