@@ -120,6 +120,11 @@ typedef struct rick_plan_desc {
    * global plane index), so the shards' images add up to the whole image. */
   int w_first;
   int w_count;
+  /* NORMALIZE_UVW (gridding.c:21-83): every gridding call first normalises the
+   * rows' u, v, w in place on the device (the rows passed to rick_plan_grid /
+   * rick_plan_image are rewritten, as the reference rewrites its data arrays;
+   * rick_plan_image_host rewrites only its device copies). */
+  int normalize_uvw;
 } rick_plan_desc;
 
 typedef struct rick_plan_stats {
@@ -210,6 +215,17 @@ int rick_wstack_noalloc(int num_w_planes, uint64_t num_points, uint32_t freq_per
                         int grid_size_x, int grid_size_y, double *grid, void *stream);
 int rick_wstack_noalloc_capacity(int num_w_planes, int grid_size_x, int grid_size_y,
                                  uint64_t *max_rows);
+
+/* NORMALIZE_UVW of gridding.c:21-83 on device rows, in place, asynchronous on
+ * `stream`: u, v -> (x + maxg) / (2 maxg) with maxg = 1.001 * the largest
+ * |extremum| of u and v, w -> (w - min w) / (max w - min w), the extrema
+ * taken over the rows with minima starting at 1e20 and maxima at 0 as in the
+ * reference.  scratch: device memory of RICK_NORMALIZE_SCRATCH bytes, 8-byte
+ * aligned; when the call has run, its first 7 doubles are min u, min v, min w,
+ * max u, max v, max w and maxg. */
+#define RICK_NORMALIZE_SCRATCH 128
+int rick_normalize_uvw(uint64_t nrows, double *uu, double *vv, double *ww, void *scratch,
+                       void *stream);
 
 /* ---- 4. Batched imaging -------------------------------------------------
  * No counterpart in the reference (one rank images one dataset per run).  Many

@@ -53,6 +53,8 @@ def lib():
         L.oracle_phase_correction.restype = C.c_int
         L.oracle_sector0_rows.argtypes = [_dp, C.c_uint64, C.c_int, C.c_int, C.c_int, _u64p]
         L.oracle_sector0_rows.restype = C.c_uint64
+        L.oracle_normalize_uvw.argtypes = [C.c_uint64, _dp, _dp, _dp, _dp]
+        L.oracle_normalize_uvw.restype = None
         L.oracle_make_gauss_table.argtypes = [_dp, C.c_int]
         L.oracle_make_kb_table.argtypes = [_dp, C.c_int]
         _lib = L
@@ -209,3 +211,40 @@ def ref_sector0_rows(vv, nmeasures_read, nx, ny, w_support):
     rows = np.array([sectors[0][i] for i in range(n)], dtype=np.uint64)
     del double_half
     return rows[::-1].copy()
+
+
+def normalize_uvw(uu, vv, ww):
+    """gridding.c:21-83 (NORMALIZE_UVW) restated: normalised copies of u, v, w
+    and the extrema (min u, v, w, max u, v, w, maxg)."""
+    u, v, w = (np.array(x, dtype=np.float64, copy=True) for x in (uu, vv, ww))
+    ext = np.zeros(7)
+    lib().oracle_normalize_uvw(len(u), u, v, w, ext)
+    return u, v, w, ext
+
+
+def ref_normalize_uvw(uu, vv, ww, nx=64, ny=64, w_support=7):
+    """The reference's own gridding() built with NORMALIZE_UVW (oracle/_ref/
+    libref_norm.so), one rank, one thread: the rows it normalises in place
+    (the sector gridding it calls afterwards is stubbed out)."""
+    path = os.path.join(HERE, "_ref", "libref_norm.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"reference build missing: {path} (run `make -C oracle ref`)")
+    L = C.CDLL(path, mode=C.RTLD_LOCAL)
+    u, v, w = (np.array(x, dtype=np.float64, copy=True) for x in (uu, vv, ww))
+
+    class FileData(C.Structure):  # allvars.h:150-158
+        _fields_ = [("uu", C.c_void_p), ("vv", C.c_void_p), ("ww", C.c_void_p),
+                    ("weights", C.c_void_p), ("visreal", C.c_void_p), ("visimg", C.c_void_p)]
+    data = FileData.in_dll(L, "data")
+    data.uu, data.vv, data.ww = u.ctypes.data, v.ctypes.data, w.ctypes.data
+    C.c_int.in_dll(L, "param").value = 1                  # param.num_threads (first field)
+    C.c_uint.in_dll(L, "metaData").value = len(u)         # meta.Nmeasures (first field)
+    C.c_uint.in_dll(L, "nsectors").value = 1
+    C.c_int.in_dll(L, "yaxis").value = ny
+    dx = 1.0 / nx
+    C.c_double.in_dll(L, "dx").value = dx
+    C.c_double.in_dll(L, "w_supporth").value = float((w_support - 1) // 2) * dx
+    L.gridding.argtypes = []
+    L.gridding.restype = None
+    L.gridding()
+    return u, v, w

@@ -10,6 +10,7 @@
  *   - kernel tables        w-stacking.cu:28-89  (Gaussian, Kaiser-Bessel)
  *   - wstack (CPU branch)  w-stacking.cu:211-270, 438-536
  *   - phase_correction     phase_correction.cu:97-102, 185-250 (PHASE_ON)
+ *   - NORMALIZE_UVW        gridding.c:21-83 (one rank)
  *   - one-rank row choice  init.c:335-340 (last 1000 rows dropped),
  *                          gridding.c:139-188 (sector-0 membership incl. the
  *                          v-halo rule), gridding_cpu.c:118 (reverse packing)
@@ -279,5 +280,40 @@ void oracle_pack_rows(const uint64_t *rows, uint64_t nrows, uint32_t nchan, uint
     memcpy(weightss + r * npol, weights + i * npol, npol * sizeof(float));
     memcpy(visreals + r * nv, vis_re + i * nv, nv * sizeof(float));
     memcpy(visimgs + r * nv, vis_im + i * nv, nv * sizeof(float));
+  }
+}
+
+/* NORMALIZE_UVW of gridding.c:21-83 for one rank, in place.  The extrema start
+ * at 1e20 (minima) and 0 (maxima) as in the reference, so a maximum is never
+ * below 0; u and v map to (x + maxg) / (2 maxg) with maxg = 1.001 * the largest
+ * |extremum| of u and v, w to (w - wmin) / (wmax - wmin).  extrema[0..6] =
+ * min u, min v, min w, max u, max v, max w, maxg.  (Rows whose coordinates are
+ * NaN make the reference's result depend on the row order; they are not
+ * supported here.) */
+void oracle_normalize_uvw(uint64_t n, double *uu, double *vv, double *ww, double *extrema)
+{
+  double mnu = 1e20, mnv = 1e20, mnw = 1e20, mxu = 0.0, mxv = 0.0, mxw = 0.0;
+  for (uint64_t i = 0; i < n; i++) {
+    mnu = uu[i] < mnu ? uu[i] : mnu;
+    mnv = vv[i] < mnv ? vv[i] : mnv;
+    mnw = ww[i] < mnw ? ww[i] : mnw;
+    mxu = uu[i] > mxu ? uu[i] : mxu;
+    mxv = vv[i] > mxv ? vv[i] : mxv;
+    mxw = ww[i] > mxw ? ww[i] : mxw;
+  }
+  const double offset = 0.001;
+  const double ming = fmax(fabs(mnu), fabs(mnv));
+  double maxg = fmax(fabs(mxu), fabs(mxv));
+  maxg = maxg > ming ? maxg : ming;
+  maxg = maxg + offset * maxg;
+  for (uint64_t i = 0; i < n; i++) {
+    uu[i] = (uu[i] + maxg) / (2.0 * maxg);
+    vv[i] = (vv[i] + maxg) / (2.0 * maxg);
+    ww[i] = (ww[i] - mnw) / (mxw - mnw);
+  }
+  if (extrema) {
+    extrema[0] = mnu; extrema[1] = mnv; extrema[2] = mnw;
+    extrema[3] = mxu; extrema[4] = mxv; extrema[5] = mxw;
+    extrema[6] = maxg;
   }
 }

@@ -13,4 +13,15 @@ typedef long MPI_Aint;
 typedef int  MPI_Request;
 typedef int  MPI_Datatype;
 typedef int  MPI_Info;
+typedef int  MPI_Op;
+/* gridding.c's NORMALIZE_UVW block reduces its extrema over the ranks; with one
+ * rank and MPI_IN_PLACE that reduction leaves the buffers as they are
+ * (stub/ref_norm_stubs.c). */
+#define MPI_IN_PLACE   ((void *)1)
+#define MPI_DOUBLE     ((MPI_Datatype)0)
+#define MPI_MIN        ((MPI_Op)0)
+#define MPI_MAX        ((MPI_Op)1)
+#define MPI_COMM_WORLD ((MPI_Comm)0)
+int MPI_Allreduce(const void *sendbuf, void *recvbuf, int count, MPI_Datatype datatype, MPI_Op op,
+                  MPI_Comm comm);
 #endif

@@ -52,7 +52,7 @@ class PlanDesc(C.Structure):
                 ("w_support", C.c_int), ("kernel", C.c_int), ("precision", C.c_int),
                 ("phase_on", C.c_int), ("device", C.c_int), ("max_rows", C.c_uint64),
                 ("freq_per_chan", C.c_uint32), ("polarizations", C.c_uint32),
-                ("w_first", C.c_int), ("w_count", C.c_int)]
+                ("w_first", C.c_int), ("w_count", C.c_int), ("normalize_uvw", C.c_int)]
 
 
 class PlanStats(C.Structure):
@@ -154,6 +154,7 @@ def lib():
     L.rick_server_wait.argtypes = [_vp, C.c_uint64, C.c_double, C.POINTER(JobResult)]
     L.rick_server_get_stats.argtypes = [_vp, C.POINTER(ServerStats)]
     L.rick_server_destroy.argtypes = [_vp]
+    L.rick_normalize_uvw.argtypes = [C.c_uint64, _vp, _vp, _vp, _vp, _vp]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
     L.rick_launch_count.argtypes = []
     L.rick_launch_count.restype = C.c_ulonglong
@@ -165,7 +166,7 @@ def lib():
                "rick_batch_run", "rick_batch_get_tuning", "rick_batch_get_stats",
                "rick_batch_destroy", "rick_batch_kernels_per_run", "rick_server_create",
                "rick_server_submit", "rick_server_wait", "rick_server_get_stats",
-               "rick_server_destroy"]:
+               "rick_server_destroy", "rick_normalize_uvw"]:
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L
@@ -282,14 +283,15 @@ class Plan:
     """Device-resident imaging plan (rick_plan_* in include/rick_b200.h)."""
 
     def __init__(self, geom: Geometry, max_rows: int, freq_per_chan: int, polarizations: int,
-                 device: int = -1, planes: Optional[tuple] = None):
-        """``planes=(w_first, w_count)`` makes the plan one w-plane shard of the cube."""
+                 device: int = -1, planes: Optional[tuple] = None, normalize_uvw: bool = False):
+        """``planes=(w_first, w_count)`` makes the plan one w-plane shard of the cube;
+        ``normalize_uvw`` normalises the rows in place first (gridding.c:21-83)."""
         self.geom = geom
         w_first, w_count = planes if planes is not None else (0, 0)
         self.desc = PlanDesc(geom.grid_size_x, geom.grid_size_y, geom.num_w_planes,
                              geom.w_support, KERNELS[geom.kernel], PRECISIONS[geom.precision],
                              int(geom.phase_on), device, max_rows, freq_per_chan, polarizations,
-                             w_first, w_count)
+                             w_first, w_count, int(bool(normalize_uvw)))
         h = _vp()
         check(lib().rick_plan_create(C.byref(h), C.byref(self.desc)), "rick_plan_create")
         self._h = h
@@ -521,6 +523,14 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def normalize_uvw(nrows, uu, vv, ww, scratch, stream=None):
+    """gridding.c:21-83 in place on device rows (include/rick_b200.h);
+    ``scratch``: a CUDA tensor of >= 128 bytes, its first 7 float64 values are
+    then min u, v, w, max u, v, w and maxg."""
+    check(lib().rick_normalize_uvw(nrows, _ptr(uu), _ptr(vv), _ptr(ww), _ptr(scratch),
+                                   _stream(stream)), "rick_normalize_uvw")
 
 
 def resolution_of(meta: dict) -> float:

@@ -12,9 +12,10 @@
  *     WRITE_IMAGE          (fourier_transform.c:281-292) <i>fft_real.bin, <i>fft_img.bin
  *   write_result         (result.c:6-53)   stage times, timings.dat
  *
- * The gridding kernel, precision form and PHASE_ON are compile-time macros in
- * the reference; here they are optional paramfile keys (kernel, precision,
- * phase_on) or the RICK_KERNEL / RICK_PRECISION / RICK_PHASE_ON environment
+ * The gridding kernel, precision form, PHASE_ON and NORMALIZE_UVW are
+ * compile-time macros in the reference; here they are optional paramfile keys
+ * (kernel, precision, phase_on, normalize_uvw) or the RICK_KERNEL /
+ * RICK_PRECISION / RICK_PHASE_ON / RICK_NORMALIZE_UVW environment
  * variables, defaulting to the reference Makefile's KAISERBESSEL, FP64, on.
  * Errors print like shutdown_wstacking (main.c:6-28) and exit with the code.
  */
@@ -32,7 +33,7 @@
 
 typedef struct {
   int num_threads, ndatasets, grid_size_x, grid_size_y, num_w_planes, w_support;
-  int kernel, precision, phase_on;
+  int kernel, precision, phase_on, normalize_uvw;
   char datapath[MAX_DATASETS][NAME_LEN];
   char ufile[NAME_LEN], vfile[NAME_LEN], wfile[NAME_LEN], weightsfile[NAME_LEN];
   char visrealfile[NAME_LEN], visimgfile[NAME_LEN], metafile[NAME_LEN];
@@ -96,6 +97,7 @@ static int read_params(const char *fname, params_t *p) {
     else if (!strcmp(k, "kernel")) p->kernel = kernel_code(v);
     else if (!strcmp(k, "precision")) p->precision = !strcmp(v, "mixed") ? RICK_PREC_MIXED : RICK_PREC_FP64;
     else if (!strcmp(k, "phase_on")) p->phase_on = atoi(v) != 0;
+    else if (!strcmp(k, "normalize_uvw")) p->normalize_uvw = atoi(v) != 0;
     else if (!strncmp(k, "Datapath", 8)) {
       const int i = atoi(k + 8);
       if (i >= 1 && i <= MAX_DATASETS) strcpy(p->datapath[i - 1], v);
@@ -106,6 +108,7 @@ static int read_params(const char *fname, params_t *p) {
   if ((e = getenv("RICK_KERNEL"))) p->kernel = kernel_code(e);
   if ((e = getenv("RICK_PRECISION"))) p->precision = !strcmp(e, "mixed") ? RICK_PREC_MIXED : RICK_PREC_FP64;
   if ((e = getenv("RICK_PHASE_ON"))) p->phase_on = !(strcmp(e, "0") == 0 || strcmp(e, "off") == 0);
+  if ((e = getenv("RICK_NORMALIZE_UVW"))) p->normalize_uvw = !(strcmp(e, "0") == 0 || strcmp(e, "off") == 0);
   if (p->ndatasets < 1 || p->ndatasets > MAX_DATASETS || p->grid_size_x <= 0 ||
       p->grid_size_y <= 0 || p->num_w_planes <= 0 || p->w_support <= 0 || p->kernel < 0)
     return RICK_ERR_IN_PARAMFILE;
@@ -189,6 +192,7 @@ int main(int argc, char **argv) {
     d.kernel = P.kernel;
     d.precision = P.precision;
     d.phase_on = P.phase_on;
+    d.normalize_uvw = P.normalize_uvw;
     d.device = 0;
     d.max_rows = nm ? nm : 1;
     d.freq_per_chan = M.freq_per_chan;

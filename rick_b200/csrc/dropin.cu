@@ -296,7 +296,8 @@ int rick_kernel_names(const char **names, int max_names) {
                             "k_fft_rows",         "k_fft_cols_image",   "k_phase_sum",
                             "k_export_cube",      "k_import_cube",      "k_bin_count_batch",
                             "k_bin_scatter_batch", "k_grid_tiles_batch", "k_zero_split_tiles_batch",
-                            "k_fft_rows_multi",   "k_fft_cols_multi"};
+                            "k_fft_rows_multi",   "k_fft_cols_multi",   "k_uvw_init",
+                            "k_uvw_extrema",      "k_uvw_normalize"};
   const int n = (int)(sizeof(k) / sizeof(k[0]));
   for (int i = 0; i < n && i < max_names; i++) names[i] = k[i];
   return n;

@@ -138,6 +138,7 @@ struct rick_plan {
   uint64_t rows_cap = 0;
   double *d_img = nullptr;     // [2*Ny*Nx] image staging for host calls
   double *d_stage = nullptr;   // conversion staging for mixed import/export
+  void *d_norm = nullptr;      // NORMALIZE_UVW scratch (extrema)
   size_t stage_bytes = 0;
   uint64_t last_rows = 0;
   size_t device_bytes = 0;
@@ -326,6 +327,9 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
   fill_geometry(p, dx, dw, select);
   for (int k = 0; k < RICK_NUM_STAGES; k++) p->ran[k] = false;
   RICK_TRY(mark(p, p->ev[0], st));
+  if (p->d.normalize_uvw && nrows)  // gridding.c:21-83, in place
+    RICK_TRY(normalize_uvw(nrows, const_cast<double *>(uu), const_cast<double *>(vv),
+                           const_cast<double *>(ww), p->d_norm, st));
   RICK_CUDA(cudaMemsetAsync(p->s.counters, 0, kNumCounters * sizeof(uint64_t), st));
   const uint32_t chunk = choose_chunk(nrows);
   RICK_TRY(bin_rows(p->g, p->d.kernel, p->d.precision, nrows, uu, vv, ww, weight, vis_re, vis_im,
@@ -478,6 +482,7 @@ int rick_plan_create(rick_plan **out, const rick_plan_desc *desc) {
     if (st == RICK_OK) st = dev_alloc(p, ptr, bytes);
   };
   A(&p->cube, p->cube_vals * p->val_bytes);
+  if (desc->normalize_uvw) A(&p->d_norm, RICK_NORMALIZE_SCRATCH);
   A((void **)&p->s.bin_count, (nbins + 1) * 4);
   A((void **)&p->s.bin_cursor, nbins * 4);
   A((void **)&p->s.item_off, (nbins + 1) * 4);
@@ -573,7 +578,7 @@ int rick_plan_destroy(rick_plan *p) {
   if (p->fft) cufftDestroy(p->fft);
   void *ptrs[] = {p->cube, p->s.bin_count, p->s.bin_cursor, p->s.item_off, p->s.scan_tmp,
                   p->s.counters, p->s.records, p->s.table, p->d_lm, p->fft_work, p->h_rows_d,
-                  p->d_img, p->d_stage, p->f.rowmask, p->f.rowlist, p->f.counts,
+                  p->d_img, p->d_stage, p->d_norm, p->f.rowmask, p->f.rowlist, p->f.counts,
                   p->f.tw_x64, p->f.tw_y64, p->f.tw_x32, p->f.tw_y32, p->f.blocked,
                   p->f.tilemask, p->d_job, p->d_fft_tabs, p->d_mask_base};
   for (void *q : ptrs)

@@ -200,6 +200,9 @@ int phase_sum(int precision, const void *cube, int xaxis, int yaxis, int nw, int
               int nw_total, const double *ltab, const double *mtab, double wmin, double wmax,
               double norm, int phase_on, int accumulate, double *img_re, double *img_im,
               cudaStream_t st);
+// gridding.c:21-83 on device rows (uvw.cu); scratch: RICK_NORMALIZE_SCRATCH bytes.
+int normalize_uvw(uint64_t n, double *uu, double *vv, double *ww, void *scratch,
+                  cudaStream_t st);
 int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *tmp,
                        cudaStream_t st);
 uint64_t scan_tmp_words(uint64_t n);

@@ -1,6 +1,8 @@
 """The oracle, pinned: against the golden fixtures (made by the reference's own
 compiled code, tests/golden/make_golden.py) and, where the reference build is
 present, against the reference bit for bit.  CPU only."""
+import os
+
 import numpy as np
 import pytest
 
@@ -136,3 +138,30 @@ def test_row_selection_vs_reference(grid, sup):
     a = O.sector0_rows(vv, 5000, grid, grid, sup)
     b = O.ref_sector0_rows(vv, 4000, grid, grid, sup)
     assert np.array_equal(a, b)
+
+
+def _uvw_cases():
+    rng = np.random.default_rng(3)
+    n = 5000
+    for case in range(4):
+        u = rng.normal(0, 3000, n); v = rng.normal(-100, 2000, n); w = rng.normal(5, 50, n)
+        if case == 1:
+            w = -np.abs(w) - 1            # every w negative: max w stays at its start value 0
+        if case == 2:
+            u, v = np.abs(u) + 10, np.abs(v) + 5
+        if case == 3:
+            u, v = -np.abs(u), -np.abs(v)
+        yield u, v, w
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(O.__file__), "_ref",
+                                                    "libref_norm.so")),
+                    reason="reference build (oracle/_ref) not present")
+def test_normalize_uvw_matches_reference_bit_for_bit():
+    """gridding.c:21-83 through the reference's own gridding() (NORMALIZE_UVW,
+    one rank) against the oracle's restatement."""
+    for u, v, w in _uvw_cases():
+        a = O.normalize_uvw(u, v, w)
+        b = O.ref_normalize_uvw(u, v, w)
+        for x, y in zip(a[:3], b):
+            assert np.array_equal(x, y)
