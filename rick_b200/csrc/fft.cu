@@ -526,15 +526,23 @@ template <typename T> struct ColJob {
 };
 
 // Shared memory of one block of the column pass: NB column buffers per row
-// group, the per-pixel phase steps (RECUR) and the row masks of 2*PP planes.
+// group, the per-pixel phase steps (RECUR; complex in the accumulation type T)
+// and the row masks of 2*PP planes.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __host__ __device__ constexpr size_t cols_smem_bytes(int rpc) {
   return (size_t)rpc * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(typename V2<T>::t) *
              (DB ? 2 : 1) * PP +
-         (RECUR ? (size_t)rpc * (1 << LOGN) * 16 : 0) + 2 * PP * (size_t)((1 << LOGN) / 32) * 4;
+         (RECUR ? (size_t)rpc * (1 << LOGN) * sizeof(typename V2<T>::t) : 0) +
+         2 * PP * (size_t)((1 << LOGN) / 32) * 4;
 }
 
-// Columns base..base+rpc-1 (one per row group) of one job.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// Columns base..base+rpc-1 (one per row group) of one job.  The pixel sums,
+// the phase factors and the per-pixel steps are kept in the FFT's type: FP64
+// for the plain form; FP32 for the mixed form, whose phase arguments (and
+// their sincos) stay FP64 -- only the unit-modulus factors are rounded.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base,
                                              const ColJob<T> &J) {
@@ -548,8 +556,8 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   const uint32_t *__restrict__ counts = J.counts;
   const double *__restrict__ mtab = J.mtab;
   V *sbase = s + grp * NB * LEN;  // buffers [set][pp]: set = cur (DB), pp < PP
-  double2 *tables = reinterpret_cast<double2 *>(s + rpc * NB * LEN);
-  double2 *sstep = tables + grp * N;  // RECUR only
+  V *tables = s + rpc * NB * LEN;
+  V *sstep = tables + grp * N;  // RECUR only
   // row masks of the planes of the next two sets (2 * PP slots)
   uint32_t *smask = reinterpret_cast<uint32_t *>(tables + (RECUR ? rpc * N : 0));
   const bool phase = J.phase_on && J.nw_total > 1;
@@ -606,9 +614,10 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   };
   const double dwstep = __dmul_rn(twopi, J.dw);
   const double l = active ? J.ltab[n] : 0.0;
-  double acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
+  T acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
 #pragma unroll
-  for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = 0.0;
+  for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = (T)0;
+  const T norm = (T)J.norm;  // 1/(Nx*Ny): a power of two, exact in FP32
   int cur[PP], nxt[PP];
   next_set(-1, cur);
   next_set(cur[PP - 1], nxt);
@@ -620,7 +629,10 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
       const int m = t + q * G;
       double sn, cs;
       sincos(__dmul_rn(dwstep, __dsub_rn(root_of(l, m), 1.0)), &sn, &cs);
-      sstep[m] = make_double2(cs, sn);
+      V st;
+      st.x = (T)cs;
+      st.y = (T)sn;
+      sstep[m] = st;
     }
   }
   __syncthreads();
@@ -663,25 +675,25 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int m = t + q * G;
-        const double p = __dmul_rn(J.norm, (double)x[pp][q].re);
-        const double qq = __dmul_rn(J.norm, (double)x[pp][q].im);
+        const T p = mul_rn(norm, x[pp][q].re);
+        const T qq = mul_rn(norm, x[pp][q].im);
         if (phase) {
           if (anchor) {
             const double root = root_of(l, m);
             double sn, cs;
             sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
             const double amp = J.dwnorm * root;
-            ph_re[q] = cs * amp;
-            ph_im[q] = sn * amp;
+            ph_re[q] = (T)(cs * amp);
+            ph_im[q] = (T)(sn * amp);
           } else {
-            const double2 st = sstep[m];
-            double sr = st.x, si = st.y;
+            const V st = sstep[m];
+            T sr = st.x, si = st.y;
             for (int g2 = 1; g2 < gap; g2++) {
-              const double tr = sr * st.x - si * st.y;
+              const T tr = sr * st.x - si * st.y;
               si = sr * st.y + si * st.x;
               sr = tr;
             }
-            const double tr = ph_re[q] * sr - ph_im[q] * si;
+            const T tr = ph_re[q] * sr - ph_im[q] * si;
             ph_im[q] = ph_re[q] * si + ph_im[q] * sr;
             ph_re[q] = tr;
           }
@@ -707,8 +719,8 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int m = t + q * G;
-      J.img_re[(uint64_t)m * nx + n] = acc_re[q];
-      J.img_im[(uint64_t)m * nx + n] = acc_im[q];
+      J.img_re[(uint64_t)m * nx + n] = (double)acc_re[q];
+      J.img_im[(uint64_t)m * nx + n] = (double)acc_im[q];
     }
   }
   __syncthreads();  // sstep / smask are rewritten for the next column
