@@ -156,7 +156,7 @@ def algorithmic_bytes(n_rows, nvis, npol, records, nx, ny, nw, val_bytes, fft_ro
     the FP64 image; the cube is not cleared (stage cube_zero only clears the
     row/tile masks and the split tiles)."""
     g = 2 * nw * nx * ny * val_bytes                 # the cube
-    rec = 40 * records                                # binned row records
+    rec = 32 * records                                # binned row records
     out = {
         "bin_count": 24 * n_rows,                                   # u,v,w read once
         "bin_scatter": 8 * nvis + n_rows * (24 + 4 * npol) + rec,   # vis+uvw+weights in, records out

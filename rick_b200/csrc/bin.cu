@@ -250,10 +250,8 @@ __device__ __forceinline__ void scatter_rows(
   RecF64 r;
   r.sre = my_re;
   r.sim = my_im;
-  r.fu = p.pu - (double)p.gu;  // exact (Sterbenz)
-  r.fv = p.pv - (double)p.gv;
-  r.gu = p.gu;
-  r.gv = p.gv;
+  r.pu = p.pu;
+  r.pv = p.pv;
 #pragma unroll
   for (int s = 0; s < 4; s++) {
     const unsigned peers = __match_any_sync(kFull, bins[s]);

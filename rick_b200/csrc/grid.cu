@@ -56,12 +56,15 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
     const bool valid = r < r1;
     RecF64 q;
     if (valid) q = rec[r];
-    else { q.sre = q.sim = q.fu = q.fv = 0.0; q.gu = q.gv = -1000000; }
+    else q.sre = q.sim = q.pu = q.pv = 0.0;
+    // the cell and the exact fraction (Sterbenz) of the record's position
+    const int qgu = valid ? (int)q.pu : -1000000, qgv = valid ? (int)q.pv : -1000000;
+    const double qfu = __dsub_rn(q.pu, (double)(int)q.pu), qfv = __dsub_rn(q.pv, (double)(int)q.pv);
     double wu = 0.0, wv = 0.0;
     if (valid && (int)d < g.support) {
       const double off = __dadd_rn((double)((int)d - g.half), 0.5);
-      const double ud = __dsub_rn(off, q.fu);  // == (j + 0.5) - pos_u exactly
-      const double vd = __dsub_rn(off, q.fv);
+      const double ud = __dsub_rn(off, qfu);  // == (j + 0.5) - pos_u exactly
+      const double vd = __dsub_rn(off, qfv);
       if (hi) {
         wu = exp(-__dmul_rn(ud, ud) * kStd22);
         wv = exp(-__dmul_rn(vd, vd) * kStd22);
@@ -74,12 +77,12 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
         wv = s_tab[min(kk, ntab - 1)];
       }
     }
-    const int j = q.gu - g.half + (int)d;
+    const int j = qgu - g.half + (int)d;
     const bool col_ok = valid && (int)d < g.support && j >= 0 && j < g.nx && j >= x0 && j < x0 + kTile;
     if (rowmask && valid && d == 0) {
       // grid rows of this tile the record's footprint reaches
-      const int lo = max(max(q.gv - g.half, 0), y0);
-      const int hi_r = min(min(q.gv + g.half, g.ny - 1), y0 + kTile - 1);
+      const int lo = max(max(qgv - g.half, 0), y0);
+      const int hi_r = min(min(qgv + g.half, g.ny - 1), y0 + kTile - 1);
       if (lo <= hi_r) {
         const uint32_t span = (uint32_t)(hi_r - lo + 1);
         const uint32_t bits = (span >= 32u ? 0xffffffffu : ((1u << span) - 1u)) << (lo - y0);
@@ -89,7 +92,7 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
     const double su = hi ? gnorm * wu : wu;
     for (int e = 0; e < g.support; e++) {
       const double wve = __shfl_sync(kFull, wv, grp_base + e);
-      const int k = q.gv - g.half + e;
+      const int k = qgv - g.half + e;
       if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
         const double cw = su * wve;
         const int cell = (k - y0) * kPitch + (j - x0);

@@ -61,12 +61,13 @@ struct Geometry {
   uint64_t nbins() const { return (uint64_t)nw * ntx * nty; }
 };
 
-// Binned row record of the FP64 form.  fu, fv are pos - (int)pos, exact in
-// FP64, so (d + 0.5) - f rounds to the reference's (j + 0.5) - pos exactly.
-struct __align__(8) RecF64 {
+// Binned row record (32 bytes: one DRAM sector, two 16-byte loads).  pu, pv
+// are the FP64 pixel positions u/dx, v/dx of w-stacking.cu:143-144; the
+// gridder re-derives the cell (int)pos and the fraction pos - (int)pos, exact
+// in FP64, so (d + 0.5) - f rounds to the reference's (j + 0.5) - pos exactly.
+struct __align__(16) RecF64 {
   double sre, sim;   // sum over channels and polarisations of weight*vis
-  double fu, fv;     // fractional pixel position
-  int gu, gv;        // integer pixel position (truncated toward zero)
+  double pu, pv;     // pixel position
 };
 
 // Device scratch owned by a plan.
