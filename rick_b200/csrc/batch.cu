@@ -53,7 +53,7 @@ struct Layout {
   std::vector<uint64_t> cube, blocked, lm, table;  // per job
   std::vector<int> tw_log;                          // FFT lengths with twiddles
   std::map<int, uint64_t> tw;                       // log -> offset
-  uint64_t jobs = 0, row_units = 0, bin_base = 0, mask_base = 0, fft_tabs = 0;
+  uint64_t jobs = 0, row_units = 0, bin_base = 0, mask_base = 0, fft_tabs = 0, sc_tabs = 0;
   uint64_t rowmask = 0, tilemask = 0, rowlist = 0, counts = 0;
   uint64_t bin_count = 0, bin_cursor = 0, item_off = 0, scan_tmp = 0, counters = 0, records = 0;
   uint64_t total = 0;
@@ -126,6 +126,7 @@ int plan_layout(const std::vector<rick_job_desc> &jobs, int precision, Layout &L
   L.bin_base = take(4ull * (n + 1));
   L.mask_base = take(8ull * (n + 1));
   L.fft_tabs = take(4ull * (3 * n + 2));  // fft_units [n+1], col_jobs [n], col_units [n+1]
+  L.sc_tabs = take(8ull * (n + 1) + 4ull * n);  // sc_units [n+1] (u64), sc_jobs [n] (u32)
   L.rowmask = take(4 * L.total_mask_words);
   L.tilemask = take(4 * L.total_tile_words);
   L.rowlist = take(4 * L.total_list);
@@ -294,8 +295,38 @@ int build_tables(rick_batch *b, cudaStream_t st) {
   RICK_CUDA(cudaMemcpyAsync(A + L.mask_base, mask_base.data(), 8 * (n + 1), cudaMemcpyHostToDevice,
                             st));
   RICK_CUDA(cudaMemcpyAsync(A + L.fft_tabs, tabs.data(), 4 * tabs.size(), cudaMemcpyHostToDevice, st));
-
+  // sample-pass schedules: the jobs grouped by (lanes per row, 16-byte loads)
   BatchLaunch &bl = b->bl;
+  {
+    std::vector<uint64_t> sc_units(n + 1, 0);
+    std::vector<uint32_t> sc_jobs(n, 0);
+    int k = 0;
+    uint64_t acc = 0;
+    bl.n_sc = 0;
+    for (int v4 = 1; v4 >= 0; v4--)
+      for (int lanes = 1; lanes <= 32; lanes *= 2) {
+        const int lo = k;
+        uint64_t units = 0;
+        for (int j = 0; j < n; j++) {
+          if (hj[j].scatter_v4 != v4 || hj[j].scatter_lanes != lanes) continue;
+          sc_jobs[k] = (uint32_t)j;
+          sc_units[k] = acc;
+          const uint64_t u = (hj[j].nrows + 31) / 32;
+          acc += u;
+          units += u;
+          k++;
+        }
+        if (k > lo && units > 0) bl.sc[bl.n_sc++] = ScatterClass{lanes, v4 != 0, lo, k, units};
+      }
+    sc_units[n] = acc;
+    RICK_CUDA(cudaMemcpyAsync(A + L.sc_tabs, sc_units.data(), 8 * (n + 1), cudaMemcpyHostToDevice,
+                              st));
+    RICK_CUDA(cudaMemcpyAsync(A + L.sc_tabs + 8 * (n + 1), sc_jobs.data(), 4 * n,
+                              cudaMemcpyHostToDevice, st));
+    bl.sc_units = (const uint64_t *)(A + L.sc_tabs);
+    bl.sc_jobs = (const uint32_t *)(A + L.sc_tabs + 8 * (n + 1));
+  }
+
   bl.jobs = (const BatchJob *)(A + L.jobs);
   bl.njobs = n;
   bl.u.row_units = (const uint64_t *)(A + L.row_units);

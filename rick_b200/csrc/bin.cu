@@ -296,44 +296,28 @@ __global__ void __launch_bounds__(256)
   add_scatter_counts(gridded, nrec, counters);
 }
 
-// The same over every job of a batch; each job has its own lanes per row and
-// load width (warp-uniform: a unit is 32 rows of one job).
-__global__ void __launch_bounds__(256)
-    k_bin_scatter_batch(const BatchJob *__restrict__ jobs, int njobs,
-                        const uint64_t *__restrict__ row_units, uint64_t total_units,
+// The same over the jobs of one sample-pass schedule of a batch (lanes per row
+// G, load width V4): the k-th listed job's rows are units sc_units[k] ..
+// sc_units[k+1]-1 (a unit is 32 rows of one job).  Bounded to three blocks
+// per SM: the job lookup and the per-job geometry add registers to the
+// single-job kernel's set.
+template <int G, bool V4>
+__global__ void __launch_bounds__(256, 3)
+    k_bin_scatter_batch(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ sc_jobs,
+                        const uint64_t *__restrict__ sc_units, int lo, int hi,
                         const uint32_t *__restrict__ bin_off, uint32_t *__restrict__ bin_cursor,
                         RecF64 *__restrict__ rec, uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
   uint32_t gridded = 0, nrec = 0;
-  for (uint64_t u = warp; u < total_units; u += nwarps) {
-    const int j = batch_job_of(row_units, njobs, u);
-    const BatchJob &J = jobs[j];
+  const uint64_t u1 = sc_units[hi];
+  for (uint64_t u = sc_units[lo] + warp; u < u1; u += nwarps) {
+    const int k = lo + batch_job_of(sc_units + lo, hi - lo, u);
+    const BatchJob &J = jobs[sc_jobs[k]];
     const Geometry g = J.g;
-    const uint64_t base = (u - row_units[j]) * 32;
-#define RICK_SC(GG, VV)                                                                          \
-  scatter_rows<GG, VV>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan, J.npol, \
-                       g, base, J.bin_base, bin_off, bin_cursor, rec, gridded, nrec)
-    if (J.scatter_v4) {
-      switch (J.scatter_lanes) {
-        case 1: RICK_SC(1, true); break;
-        case 2: RICK_SC(2, true); break;
-        case 4: RICK_SC(4, true); break;
-        case 8: RICK_SC(8, true); break;
-        case 16: RICK_SC(16, true); break;
-        default: RICK_SC(32, true); break;
-      }
-    } else {
-      switch (J.scatter_lanes) {
-        case 1: RICK_SC(1, false); break;
-        case 2: RICK_SC(2, false); break;
-        case 4: RICK_SC(4, false); break;
-        case 8: RICK_SC(8, false); break;
-        case 16: RICK_SC(16, false); break;
-        default: RICK_SC(32, false); break;
-      }
-    }
-#undef RICK_SC
+    scatter_rows<G, V4>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan, J.npol,
+                        g, (u - sc_units[k]) * 32, J.bin_base, bin_off, bin_cursor, rec, gridded,
+                        nrec);
   }
   add_scatter_counts(gridded, nrec, counters);
 }
@@ -439,10 +423,34 @@ int bin_rows_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cudaStr
   k_item_count<<<blocks_items, 256, 0, st>>>(s.bin_count, nbins, max_chunk, s.item_off);
   RICK_CUDA(cudaGetLastError());
   RICK_TRY(exclusive_scan_u32(s.item_off, s.item_off, nbins + 1, s.scan_tmp, st));
-  const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((units + 7) / 8, (uint64_t)sms * 8));
-  RICK_LAUNCHED();
-  k_bin_scatter_batch<<<blocks, 256, 0, st>>>(b.jobs, b.njobs, b.u.row_units, units, s.bin_count,
-                                              s.bin_cursor, s.records, s.counters);
+  for (int c = 0; c < b.n_sc; c++) {
+    const ScatterClass &k = b.sc[c];
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((k.units + 7) / 8,
+                                                                      (uint64_t)sms * 8));
+#define RICK_SC(GG)                                                                            \
+  case GG:                                                                                     \
+    RICK_LAUNCHED();                                                                           \
+    if (k.v4)                                                                                  \
+      k_bin_scatter_batch<GG, true><<<blocks, 256, 0, st>>>(b.jobs, b.sc_jobs, b.sc_units, k.lo, \
+                                                            k.hi, s.bin_count, s.bin_cursor,    \
+                                                            s.records, s.counters);             \
+    else                                                                                       \
+      k_bin_scatter_batch<GG, false><<<blocks, 256, 0, st>>>(b.jobs, b.sc_jobs, b.sc_units,     \
+                                                             k.lo, k.hi, s.bin_count,           \
+                                                             s.bin_cursor, s.records,           \
+                                                             s.counters);                       \
+    break;
+    switch (k.lanes) {
+      RICK_SC(1)
+      RICK_SC(2)
+      RICK_SC(4)
+      RICK_SC(8)
+      RICK_SC(16)
+      RICK_SC(32)
+    }
+#undef RICK_SC
+    RICK_CUDA(cudaGetLastError());
+  }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }

@@ -224,10 +224,23 @@ __device__ __forceinline__ int batch_job_of(const U *__restrict__ base, int njob
 #endif
 
 // Batch stages: every job of the batch in one launch per kernel.
+// Jobs of one sample-pass schedule (lanes per row, 16-byte loads): entries
+// lo..hi-1 of the schedule-ordered job list.
+struct ScatterClass {
+  int lanes;
+  bool v4;
+  int lo, hi;
+  uint64_t units;  // 32-row units of the class
+};
+
 struct BatchLaunch {
   const BatchJob *jobs;    // device [njobs]
   int njobs;
   BatchUnits u;
+  const uint32_t *sc_jobs;   // device [njobs]: jobs grouped by sample-pass schedule
+  const uint64_t *sc_units;  // device [njobs + 1]: 32-row unit prefix in that order
+  int n_sc;
+  ScatterClass sc[12];
   uint64_t total_row_units;
   uint32_t total_bins;
   int max_support;
