@@ -3,9 +3,10 @@
 // Replaces convolve_g (w-stacking.cu:104-206), which scatters every footprint
 // cell of every row with two FP64 atomics straight into HBM.  Here a persistent
 // kernel takes work items (a bounded chunk of the binned records of one
-// 32x32 tile of one w-plane), accumulates their footprints in shared memory in
-// the cube's type (FP64 for the plain form, FP32 for the mixed form; weights
-// and products are formed in FP64 either way), and writes the tile once: with
+// 32x32 tile of one w-plane), accumulates their footprints in shared memory as
+// exact 64-bit fixed-point sums (weights and products formed in FP64; each
+// item scales its contributions by a power of two chosen from a bound on its
+// records, so that no sum can overflow), and writes the tile once: with
 // plain coalesced stores when the tile is
 // a single item, or with one atomic per non-zero cell when a dense tile was
 // split over several items.  The kernel weights follow w-stacking.cu:162-180:
@@ -30,6 +31,71 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
+// The shared tile: per cell and component a 64-bit two's-complement sum kept
+// as two 32-bit words, because 32-bit integer atomics are the fast shared-memory
+// atomics (about 3x the FP32 and 6x the FP64 add rate on B200).  An add puts
+// the low word in with an atomic that returns the old value; the carry out of
+// the low word goes into the high word with the high part.  Integer sums do
+// not depend on the order of the adds, so a tile's sum is reproducible.
+struct FixTile {
+  uint32_t lo_re[kTile * kPitch], hi_re[kTile * kPitch];
+  uint32_t lo_im[kTile * kPitch], hi_im[kTile * kPitch];
+};
+
+__device__ __forceinline__ void fix_add(uint32_t *lo, uint32_t *hi, long long v) {
+  const uint32_t l = (uint32_t)(unsigned long long)v;
+  const uint32_t h = (uint32_t)((unsigned long long)v >> 32);
+  const uint32_t old = atomicAdd(lo, l);
+  atomicAdd(hi, h + ((old + l) < old ? 1u : 0u));
+}
+
+__device__ __forceinline__ long long fix_get(const uint32_t *lo, const uint32_t *hi, int c) {
+  return (long long)(((unsigned long long)hi[c] << 32) | (unsigned long long)lo[c]);
+}
+
+__device__ __forceinline__ void fix_zero(FixTile *t) {
+  for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
+    t->lo_re[c] = 0u;
+    t->hi_re[c] = 0u;
+    t->lo_im[c] = 0u;
+    t->hi_im[c] = 0u;
+  }
+}
+
+// Largest |weight product| of a footprint cell: the high-precision Gaussian's
+// u factor carries norm (w-stacking.cu:256), the tables' entries are at most
+// their maximum.
+__device__ __forceinline__ double weight_bound(bool hi, const double *s_tab, int ntab) {
+  if (hi) return kStd22 / kPi;
+  double m = 0.0;
+  for (int t = 0; t < ntab; t++) m = fmax(m, fabs(s_tab[t]));
+  return m * m;
+}
+
+// Scale 2^k of an item's fixed-point sums: every |cell sum| is at most
+// bound = sum over the records of (|sre| + |sim|) * wmax < 2^e, and sums are
+// kept below 2^61 (k = 61 - e, clamped to the double exponent range).  All
+// threads take part; returns the scale, *inv = 2^-k.
+__device__ __forceinline__ double item_scale(const RecF64 *__restrict__ rec, uint32_t r0,
+                                             uint32_t r1, double wmax, double *s_red,
+                                             double *inv) {
+  double part = 0.0;
+  for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+    part += fabs(rec[r].sre) + fabs(rec[r].sim);
+  for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  double bound = 0.0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); i++) bound += s_red[i];
+  bound = bound * wmax * (1.0 + 1e-9);
+  int e = 0;
+  frexp(bound, &e);  // bound < 2^e
+  const int k = bound > 0.0 ? max(-1000, min(1000, 61 - e)) : 0;
+  __syncthreads();  // s_red is reused by the next item
+  *inv = scalbn(1.0, -k);
+  return scalbn(1.0, k);
+}
+
 // Records r0..r1 of tile (tx, ty) of plane w: footprints accumulated in the
 // shared tile (s_re, s_im, zeroed by the caller), then the tile written to the
 // cube and the rows/tile it touched marked.  LPR lanes per record (a power of
@@ -37,11 +103,12 @@ template <> struct Vec2<float> { using type = float2; };
 template <typename OutT, int LPR>
 __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32_t r0, uint32_t r1,
                                           const Geometry &g, bool hi, const double *s_tab,
-                                          int ntab, int tx, int ty, int w, bool single,
-                                          int accumulate, typename Vec2<OutT>::type *__restrict__ cube,
+                                          int ntab, double wmax, int tx, int ty, int w,
+                                          bool single, int accumulate,
+                                          typename Vec2<OutT>::type *__restrict__ cube,
                                           uint32_t *__restrict__ rowmask,
-                                          uint32_t *__restrict__ tilemask, OutT *s_re,
-                                          OutT *s_im, uint32_t *s_rows) {
+                                          uint32_t *__restrict__ tilemask, FixTile *tile,
+                                          double *s_red, uint32_t *s_rows) {
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const unsigned d = lane % LPR;                 // footprint column / row handled
   const unsigned grp_base = lane - d;            // first lane of this record's group
@@ -49,6 +116,8 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
   constexpr int kWarps = kGridThreads / 32;
   const double gnorm = kStd22 / kPi;             // w-stacking.cu:256
   const int x0 = tx * kTile, y0 = ty * kTile;
+  double inv_scale;
+  const double scale = item_scale(rec, r0, r1, wmax, s_red, &inv_scale);
 
   // Footprints of the chunk's records into the shared tile.
   for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
@@ -96,8 +165,8 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
       if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
         const double cw = su * wve;
         const int cell = (k - y0) * kPitch + (j - x0);
-        atomicAdd(&s_re[cell], (OutT)(q.sre * cw));
-        atomicAdd(&s_im[cell], (OutT)(q.sim * cw));
+        fix_add(&tile->lo_re[cell], &tile->hi_re[cell], __double2ll_rn((q.sre * cw) * scale));
+        fix_add(&tile->lo_im[cell], &tile->hi_im[cell], __double2ll_rn((q.sim * cw) * scale));
       }
     }
   }
@@ -115,7 +184,9 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
     const int gy = y0 + y, gx = x0 + x;
     if (gy >= g.ny || gx >= g.nx) continue;
     const uint64_t idx = (uint64_t)w * plane + (uint64_t)gy * g.nx + gx;
-    const OutT vr = s_re[y * kPitch + x], vi = s_im[y * kPitch + x];
+    const int cs = y * kPitch + x;
+    const OutT vr = (OutT)((double)fix_get(tile->lo_re, tile->hi_re, cs) * inv_scale);
+    const OutT vi = (OutT)((double)fix_get(tile->lo_im, tile->hi_im, cs) * inv_scale);
     if (single) {
       if (accumulate) {
         auto o = cube[idx];
@@ -154,15 +225,17 @@ __global__ void __launch_bounds__(kGridThreads)
                  uint64_t *__restrict__ counters,
                  typename Vec2<OutT>::type *__restrict__ cube, uint32_t *__restrict__ rowmask,
                  uint32_t *__restrict__ tilemask) {
-  __shared__ OutT s_re[kTile * kPitch];
-  __shared__ OutT s_im[kTile * kPitch];
+  __shared__ FixTile tile;
   __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
+  __shared__ double s_red[kGridThreads / 32];
   __shared__ uint32_t s_item, s_bin, s_first, s_nitems, s_rows;
 
   const int ntab = kIncreasePrecision * g.support;
   for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = table[t];
   const uint32_t total_items = item_off[nbins];
   const bool hi = (kernel == RICK_KERNEL_GAUSS_HI_PRECISION);
+  __syncthreads();
+  const double wmax = weight_bound(hi, s_tab, ntab);
 
   for (;;) {
     if (threadIdx.x == 0) {
@@ -177,10 +250,7 @@ __global__ void __launch_bounds__(kGridThreads)
       s_bin = bin;
       s_rows = 0;
     }
-    for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
-      s_re[c] = (OutT)0;
-      s_im[c] = (OutT)0;
-    }
+    fix_zero(&tile);
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= total_items) break;
@@ -191,8 +261,8 @@ __global__ void __launch_bounds__(kGridThreads)
     const int w = (int)(bin / ((uint32_t)g.ntx * (uint32_t)g.nty));
     const uint32_t r0 = bin_off[bin] + chunk * max_chunk;
     const uint32_t r1 = min(bin_off[bin + 1], r0 + max_chunk);
-    grid_item<OutT, LPR>(rec, r0, r1, g, hi, s_tab, ntab, tx, ty, w, s_nitems == 1, accumulate,
-                         cube, rowmask, tilemask, s_re, s_im, &s_rows);
+    grid_item<OutT, LPR>(rec, r0, r1, g, hi, s_tab, ntab, wmax, tx, ty, w, s_nitems == 1,
+                         accumulate, cube, rowmask, tilemask, &tile, s_red, &s_rows);
     __syncthreads();
   }
 }
@@ -207,14 +277,15 @@ __global__ void __launch_bounds__(kGridThreads)
                        const uint32_t *__restrict__ bin_off, const uint32_t *__restrict__ item_off,
                        uint32_t nbins, uint32_t max_chunk, uint64_t *__restrict__ counters,
                        uint32_t *__restrict__ rowmask, uint32_t *__restrict__ tilemask) {
-  __shared__ OutT s_re[kTile * kPitch];
-  __shared__ OutT s_im[kTile * kPitch];
+  __shared__ FixTile tile;
   __shared__ double s_tab[kIncreasePrecision * kMaxSupport];
+  __shared__ double s_red[kGridThreads / 32];
   __shared__ uint32_t s_item, s_bin, s_first, s_nitems, s_rows;
   __shared__ int s_job;
 
   const uint32_t total_items = item_off[nbins];
   int cur_job = -1;
+  double wmax = 0.0;
   for (;;) {
     if (threadIdx.x == 0) {
       const uint32_t item = (uint32_t)atomicAdd((unsigned long long *)&counters[kCntItemNext], 1ull);
@@ -231,10 +302,7 @@ __global__ void __launch_bounds__(kGridThreads)
       s_job = job;
       s_rows = 0;
     }
-    for (int c = threadIdx.x; c < kTile * kPitch; c += blockDim.x) {
-      s_re[c] = (OutT)0;
-      s_im[c] = (OutT)0;
-    }
+    fix_zero(&tile);
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= total_items) break;
@@ -242,10 +310,12 @@ __global__ void __launch_bounds__(kGridThreads)
     const BatchJob &J = jobs[j];
     const Geometry g = J.g;
     const int ntab = kIncreasePrecision * g.support;
+    const bool hi = J.kernel == RICK_KERNEL_GAUSS_HI_PRECISION;
     if (j != cur_job) {  // block-uniform
       for (int t = threadIdx.x; t < ntab; t += blockDim.x) s_tab[t] = J.table[t];
       cur_job = j;
       __syncthreads();
+      wmax = weight_bound(hi, s_tab, ntab);
     }
     const uint32_t bin = s_bin;
     const uint32_t lbin = bin - J.bin_base;
@@ -255,9 +325,9 @@ __global__ void __launch_bounds__(kGridThreads)
     const int w = (int)(lbin / ((uint32_t)g.ntx * (uint32_t)g.nty));
     const uint32_t r0 = bin_off[bin] + chunk * max_chunk;
     const uint32_t r1 = min(bin_off[bin + 1], r0 + max_chunk);
-    grid_item<OutT, LPR>(rec, r0, r1, g, J.kernel == RICK_KERNEL_GAUSS_HI_PRECISION, s_tab, ntab,
-                         tx, ty, w, s_nitems == 1, 0, (typename Vec2<OutT>::type *)J.cube,
-                         rowmask + J.mask_base, tilemask + J.tile_base, s_re, s_im, &s_rows);
+    grid_item<OutT, LPR>(rec, r0, r1, g, hi, s_tab, ntab, wmax, tx, ty, w, s_nitems == 1, 0,
+                         (typename Vec2<OutT>::type *)J.cube, rowmask + J.mask_base,
+                         tilemask + J.tile_base, &tile, s_red, &s_rows);
     __syncthreads();
   }
 }
