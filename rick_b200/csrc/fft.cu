@@ -146,6 +146,31 @@ __device__ __forceinline__ uint64_t blocked_index(uint32_t w, uint32_t k, uint32
 // One Stockham pass of radix R over N points held in shared memory by the N/8
 // threads of a row group (every value is read into registers before any is
 // written back, so the pass works in place).
+// The R twiddles of butterfly jm of the pass of stride Ns: w[r] =
+// exp(+2 pi i jm r / (Ns R)).  Only w[1] is read (entry (Ns-1) + jm of the
+// per-pass table, consecutive lanes reading consecutive entries; the entries a
+// column FFT reads total N/7 complex values, which stay in L1); the other
+// powers are products of it (w2 = w1^2, w4 = w2^2, w3 = w1 w2, w5 = w1 w4,
+// w6 = w2 w4, w7 = w3 w4: a few ulp, far inside the tolerances).
+template <typename T, int R>
+__device__ __forceinline__ void pass_twiddles(const typename V2<T>::t *__restrict__ twp,
+                                              Cx<T> w[R]) {
+  w[0] = {(T)1, (T)0};
+  if (R == 1) return;
+  const typename V2<T>::t a = __ldg(twp);
+  w[1] = {a.x, a.y};
+  if (R >= 4) {
+    w[2] = cmul<T>(w[1], w[1].re, w[1].im);
+    w[3] = cmul<T>(w[1], w[2].re, w[2].im);
+  }
+  if (R == 8) {
+    w[4] = cmul<T>(w[2], w[2].re, w[2].im);
+    w[5] = cmul<T>(w[1], w[4].re, w[4].im);
+    w[6] = cmul<T>(w[2], w[4].re, w[4].im);
+    w[7] = cmul<T>(w[3], w[4].re, w[4].im);
+  }
+}
+
 template <typename T, int N, int R>
 __device__ __forceinline__ void stockham_pass(typename V2<T>::t *s, int t, int Ns,
                                               const typename V2<T>::t *__restrict__ tw) {
@@ -163,27 +188,10 @@ __device__ __forceinline__ void stockham_pass(typename V2<T>::t *s, int t, int N
     const int j = t + b * G;
     const int jm = j & (Ns - 1);
     if (Ns > 1) {
-      // per-pass table: entry (Ns-1) + (r-1)*Ns + jm = exp(+2 pi i jm r / (Ns R)),
-      // so consecutive lanes read consecutive entries.  Radix 8 loads the powers
-      // 1, 2, 4 and forms 3, 5, 6, 7 as products (a few ulp, far inside 1e-12).
-      const typename V2<T>::t *twp = tw + (Ns - 1) + jm;
-      if (R == 8) {
-        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
-        const Cx<T> w1 = {a.x, a.y}, w2 = {b2.x, b2.y}, w4 = {b4.x, b4.y};
-        const Cx<T> w3 = cmul<T>(w1, w2.re, w2.im);
-        const Cx<T> w5 = cmul<T>(w1, w4.re, w4.im);
-        const Cx<T> w6 = cmul<T>(w2, w4.re, w4.im);
-        const Cx<T> w7 = cmul<T>(w3, w4.re, w4.im);
-        const Cx<T> w[8] = {{(T)1, (T)0}, w1, w2, w3, w4, w5, w6, w7};
+      Cx<T> w[R];
+      pass_twiddles<T, R>(tw + (Ns - 1) + jm, w);
 #pragma unroll
-        for (int r = 1; r < R; r++) v[b][r] = cmul<T>(v[b][r], w[r].re, w[r].im);
-      } else {
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          const typename V2<T>::t w = __ldg(twp + (r - 1) * Ns);
-          v[b][r] = cmul<T>(v[b][r], w.x, w.y);
-        }
-      }
+      for (int r = 1; r < R; r++) v[b][r] = cmul<T>(v[b][r], w[r].re, w[r].im);
     }
     Dft<T, R>::run(v[b]);
     const int idx = (j - jm) * R + jm;
@@ -212,24 +220,10 @@ __device__ __forceinline__ void stockham_last_pass(const typename V2<T>::t *s, i
   for (int b = 0; b < B; b++) {
     const int j = t + b * G;  // j < Ns, so jm = j and the output index is j + r*Ns
     if (Ns > 1) {
-      const typename V2<T>::t *twp = tw + (Ns - 1) + j;
-      if (R == 8) {
-        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
-        const Cx<T> w1 = {a.x, a.y}, w2 = {b2.x, b2.y}, w4 = {b4.x, b4.y};
-        const Cx<T> w3 = cmul<T>(w1, w2.re, w2.im);
-        const Cx<T> w5 = cmul<T>(w1, w4.re, w4.im);
-        const Cx<T> w6 = cmul<T>(w2, w4.re, w4.im);
-        const Cx<T> w7 = cmul<T>(w3, w4.re, w4.im);
-        const Cx<T> w[8] = {{(T)1, (T)0}, w1, w2, w3, w4, w5, w6, w7};
+      Cx<T> w[R];
+      pass_twiddles<T, R>(tw + (Ns - 1) + j, w);
 #pragma unroll
-        for (int r = 1; r < R; r++) v[b][r] = cmul<T>(v[b][r], w[r].re, w[r].im);
-      } else {
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          const typename V2<T>::t w = __ldg(twp + (r - 1) * Ns);
-          v[b][r] = cmul<T>(v[b][r], w.x, w.y);
-        }
-      }
+      for (int r = 1; r < R; r++) v[b][r] = cmul<T>(v[b][r], w[r].re, w[r].im);
     }
     Dft<T, R>::run(v[b]);
 #pragma unroll
@@ -279,25 +273,7 @@ __device__ __forceinline__ void stockham_pass_pp(typename V2<T>::t *const *s, in
     const int jm = j & (Ns - 1);
     Cx<T> w[R];
     w[0] = {(T)1, (T)0};
-    if (Ns > 1) {
-      const typename V2<T>::t *twp = tw + (Ns - 1) + jm;
-      if (R == 8) {
-        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
-        w[1] = {a.x, a.y};
-        w[2] = {b2.x, b2.y};
-        w[4] = {b4.x, b4.y};
-        w[3] = cmul<T>(w[1], w[2].re, w[2].im);
-        w[5] = cmul<T>(w[1], w[4].re, w[4].im);
-        w[6] = cmul<T>(w[2], w[4].re, w[4].im);
-        w[7] = cmul<T>(w[3], w[4].re, w[4].im);
-      } else {
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          const typename V2<T>::t a = __ldg(twp + (r - 1) * Ns);
-          w[r] = {a.x, a.y};
-        }
-      }
-    }
+    if (Ns > 1) pass_twiddles<T, R>(tw + (Ns - 1) + jm, w);
     const int idx = (j - jm) * R + jm;
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
@@ -323,25 +299,7 @@ __device__ __forceinline__ void stockham_last_pass_pp(typename V2<T>::t *const *
     const int j = t + b * G;  // j < Ns: the output index is j + r*Ns
     Cx<T> w[R];
     w[0] = {(T)1, (T)0};
-    if (Ns > 1) {
-      const typename V2<T>::t *twp = tw + (Ns - 1) + j;
-      if (R == 8) {
-        const typename V2<T>::t a = __ldg(twp), b2 = __ldg(twp + Ns), b4 = __ldg(twp + 3 * Ns);
-        w[1] = {a.x, a.y};
-        w[2] = {b2.x, b2.y};
-        w[4] = {b4.x, b4.y};
-        w[3] = cmul<T>(w[1], w[2].re, w[2].im);
-        w[5] = cmul<T>(w[1], w[4].re, w[4].im);
-        w[6] = cmul<T>(w[2], w[4].re, w[4].im);
-        w[7] = cmul<T>(w[3], w[4].re, w[4].im);
-      } else {
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          const typename V2<T>::t a = __ldg(twp + (r - 1) * Ns);
-          w[r] = {a.x, a.y};
-        }
-      }
-    }
+    if (Ns > 1) pass_twiddles<T, R>(tw + (Ns - 1) + j, w);
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
       Cx<T> v[R];
