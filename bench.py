@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -40,6 +41,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (non-tensor) nominal, for the column pass's compute bound
 METRIC = "imaged vis/s (1xB200) FP32-mixed vs FP64 plain @<=1e-5 rel err; p50/p99 lat"
 WORKLOAD = dict(name="c2", grid=4096, w_planes=32, kernel="kaiser_bessel", w_support=7)
 
@@ -322,6 +324,16 @@ def run_ours(args):
     if dom == "phase" and stats64.get("fft_rows", 0):
         roofline["note"] = ("column FFT + w-correction + plane sum: bound by FP64 issue and "
                             "latency (one 4096-point column of 16 warps per SM), not by HBM")
+        # algorithmic FP64 flops of the column pass: a radix-2-equivalent 5 N log2 N per
+        # column FFT of every plane (all planes hold data here), plus the w-correction's
+        # ~10 flops per pixel and plane
+        cols = nx * nw
+        flops = cols * 5.0 * ny * math.log2(ny) + 10.0 * nx * ny * nw
+        tf = flops / (stage64[dom] * 1e-3) / 1e12
+        roofline["fp64_compute"] = {"achieved_tflops": round(tf, 2), "flops": flops,
+                                    "peak_tflops_nominal": FP64_NOMINAL_TFLOPS,
+                                    "frac_of_nominal": round(tf / FP64_NOMINAL_TFLOPS, 3),
+                                    "peak_source": "nominal (B200 FP64, not measured)"}
     g8 = 2 * nw * nx * ny * 8
     in_bytes = sum(int(r.numel() * r.element_size()) for r in rows)
     pipe_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny

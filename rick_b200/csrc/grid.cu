@@ -31,26 +31,41 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-// The shared tile: per cell and component a 64-bit two's-complement sum kept
-// as two 32-bit words, because 32-bit integer atomics are the fast shared-memory
-// atomics (about 3x the FP32 and 6x the FP64 add rate on B200).  An add puts
-// the low word in with an atomic that returns the old value; the carry out of
-// the low word goes into the high word with the high part.  Integer sums do
-// not depend on the order of the adds, so a tile's sum is reproducible.
+// The shared tile: per cell and component a two's-complement fixed-point sum,
+// because 32-bit integer atomics are the fast shared-memory atomics (about 3x
+// the FP32 and 6x the FP64 add rate on B200).  The plain form keeps 64-bit
+// sums as two 32-bit words: an add puts the low word in with an atomic that
+// returns the old value, and the carry out of the low word goes into the high
+// word with the high part.  The mixed form, whose tiles are FP32, keeps one
+// 32-bit word (resolution 2^-30 of the item's bound, finer than FP32 rounding
+// of the cells that matter).  Integer sums do not depend on the order of the
+// adds, so a tile's sum is reproducible.
 struct FixTile {
   uint32_t lo_re[kTile * kPitch], hi_re[kTile * kPitch];
   uint32_t lo_im[kTile * kPitch], hi_im[kTile * kPitch];
 };
+template <typename OutT> __host__ __device__ constexpr int fix_bits() { return sizeof(OutT) == 8 ? 61 : 30; }
 
-__device__ __forceinline__ void fix_add(uint32_t *lo, uint32_t *hi, long long v) {
-  const uint32_t l = (uint32_t)(unsigned long long)v;
-  const uint32_t h = (uint32_t)((unsigned long long)v >> 32);
-  const uint32_t old = atomicAdd(lo, l);
-  atomicAdd(hi, h + ((old + l) < old ? 1u : 0u));
+template <typename OutT>
+__device__ __forceinline__ void fix_put(uint32_t *lo, uint32_t *hi, double v) {
+  if constexpr (sizeof(OutT) == 8) {
+    const long long x = __double2ll_rn(v);
+    const uint32_t l = (uint32_t)(unsigned long long)x;
+    const uint32_t h = (uint32_t)((unsigned long long)x >> 32);
+    const uint32_t old = atomicAdd(lo, l);
+    atomicAdd(hi, h + ((old + l) < old ? 1u : 0u));
+  } else {
+    (void)hi;
+    atomicAdd(lo, (uint32_t)__double2int_rn(v));
+  }
 }
 
-__device__ __forceinline__ long long fix_get(const uint32_t *lo, const uint32_t *hi, int c) {
-  return (long long)(((unsigned long long)hi[c] << 32) | (unsigned long long)lo[c]);
+template <typename OutT>
+__device__ __forceinline__ double fix_value(const uint32_t *lo, const uint32_t *hi, int c) {
+  if constexpr (sizeof(OutT) == 8)
+    return (double)(long long)(((unsigned long long)hi[c] << 32) | (unsigned long long)lo[c]);
+  else
+    return (double)(int)lo[c];
 }
 
 __device__ __forceinline__ void fix_zero(FixTile *t) {
@@ -74,10 +89,10 @@ __device__ __forceinline__ double weight_bound(bool hi, const double *s_tab, int
 
 // Scale 2^k of an item's fixed-point sums: every |cell sum| is at most
 // bound = sum over the records of (|sre| + |sim|) * wmax < 2^e, and sums are
-// kept below 2^61 (k = 61 - e, clamped to the double exponent range).  All
+// kept below 2^bits (k = bits - e, clamped to the double exponent range).  All
 // threads take part; returns the scale, *inv = 2^-k.
 __device__ __forceinline__ double item_scale(const RecF64 *__restrict__ rec, uint32_t r0,
-                                             uint32_t r1, double wmax, double *s_red,
+                                             uint32_t r1, double wmax, int bits, double *s_red,
                                              double *inv) {
   double part = 0.0;
   for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
@@ -90,7 +105,7 @@ __device__ __forceinline__ double item_scale(const RecF64 *__restrict__ rec, uin
   bound = bound * wmax * (1.0 + 1e-9);
   int e = 0;
   frexp(bound, &e);  // bound < 2^e
-  const int k = bound > 0.0 ? max(-1000, min(1000, 61 - e)) : 0;
+  const int k = bound > 0.0 ? max(-1000, min(1000, bits - e)) : 0;
   __syncthreads();  // s_red is reused by the next item
   *inv = scalbn(1.0, -k);
   return scalbn(1.0, k);
@@ -117,7 +132,7 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
   const double gnorm = kStd22 / kPi;             // w-stacking.cu:256
   const int x0 = tx * kTile, y0 = ty * kTile;
   double inv_scale;
-  const double scale = item_scale(rec, r0, r1, wmax, s_red, &inv_scale);
+  const double scale = item_scale(rec, r0, r1, wmax, fix_bits<OutT>(), s_red, &inv_scale);
 
   // Footprints of the chunk's records into the shared tile.
   for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
@@ -165,8 +180,8 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
       if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
         const double cw = su * wve;
         const int cell = (k - y0) * kPitch + (j - x0);
-        fix_add(&tile->lo_re[cell], &tile->hi_re[cell], __double2ll_rn((q.sre * cw) * scale));
-        fix_add(&tile->lo_im[cell], &tile->hi_im[cell], __double2ll_rn((q.sim * cw) * scale));
+        fix_put<OutT>(&tile->lo_re[cell], &tile->hi_re[cell], (q.sre * cw) * scale);
+        fix_put<OutT>(&tile->lo_im[cell], &tile->hi_im[cell], (q.sim * cw) * scale);
       }
     }
   }
@@ -185,8 +200,8 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
     if (gy >= g.ny || gx >= g.nx) continue;
     const uint64_t idx = (uint64_t)w * plane + (uint64_t)gy * g.nx + gx;
     const int cs = y * kPitch + x;
-    const OutT vr = (OutT)((double)fix_get(tile->lo_re, tile->hi_re, cs) * inv_scale);
-    const OutT vi = (OutT)((double)fix_get(tile->lo_im, tile->hi_im, cs) * inv_scale);
+    const OutT vr = (OutT)(fix_value<OutT>(tile->lo_re, tile->hi_re, cs) * inv_scale);
+    const OutT vi = (OutT)(fix_value<OutT>(tile->lo_im, tile->hi_im, cs) * inv_scale);
     if (single) {
       if (accumulate) {
         auto o = cube[idx];
