@@ -356,6 +356,9 @@ template <int LOGN> constexpr int block_threads() {
 // Blocks of 256 threads (lengths up to 2048) are bounded to 128 registers so
 // that two share an SM.
 template <int LOGN> constexpr int min_blocks() { return block_threads<LOGN>() <= 256 ? 2 : 1; }
+// The row pass holds no per-pixel state: 64 registers a thread, so that 1024
+// threads (4, 2 or 1 blocks) share an SM.
+template <int LOGN> constexpr int row_min_blocks() { return 1024 / block_threads<LOGN>(); }
 
 // Row pass: inverse FFT along x of the listed touched rows, from the gridded
 // cube into the column-blocked buffer.  Tiles that received no record (bit
@@ -403,7 +406,7 @@ __device__ __forceinline__ void fft_row_unit(typename V2<T>::t *s, bool active, 
 
 // One job's row pass (the plan): the job's arrays as kernel parameters.
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+__global__ void __launch_bounds__(block_threads<LOGN>(), row_min_blocks<LOGN>())
     k_fft_rows(const typename V2<T>::t *__restrict__ cube, typename V2<T>::t *__restrict__ out,
                int nx, int ny, int nty, int tmw, const uint32_t *__restrict__ tilemask,
                const uint32_t *__restrict__ rowlist, const uint32_t *__restrict__ counts,
@@ -427,7 +430,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
 // row-pass units of job j (groups of rows_per_block touched rows) are
 // fft_units[j] .. fft_units[j+1]-1.
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+__global__ void __launch_bounds__(block_threads<LOGN>(), row_min_blocks<LOGN>())
     k_fft_rows_multi(const BatchJob *__restrict__ jobs, int lo, int hi,
                const uint32_t *__restrict__ fft_units, const uint32_t *__restrict__ tilemask,
                const uint32_t *__restrict__ rowlist, const uint32_t *__restrict__ counts) {
