@@ -33,7 +33,7 @@
 
 typedef struct {
   int num_threads, ndatasets, grid_size_x, grid_size_y, num_w_planes, w_support;
-  int kernel, precision, phase_on, normalize_uvw;
+  int kernel, precision, phase_on, normalize_uvw, fits;
   char datapath[MAX_DATASETS][NAME_LEN];
   char ufile[NAME_LEN], vfile[NAME_LEN], wfile[NAME_LEN], weightsfile[NAME_LEN];
   char visrealfile[NAME_LEN], visimgfile[NAME_LEN], metafile[NAME_LEN];
@@ -64,6 +64,50 @@ static int kernel_code(const char *s) {
   if (!strcmp(s, "gauss_hi") || !strcmp(s, "GAUSS_HI_PRECISION")) return RICK_KERNEL_GAUSS_HI_PRECISION;
   if (!strcmp(s, "kaiser_bessel") || !strcmp(s, "KAISERBESSEL")) return RICK_KERNEL_KAISER_BESSEL;
   return -1;
+}
+
+/* The FITSIO output of fourier_transform.c:227-279 (parallel_real.fits,
+ * parallel_img.fits: a primary array of DOUBLE_IMG, NAXIS1 = Nx, NAXIS2 = Ny,
+ * x fastest -- the layout of the .bin images) written directly: 80-character
+ * header cards in a 2880-byte block, then big-endian IEEE doubles padded to a
+ * 2880-byte boundary.  No cfitsio is needed. */
+static int write_fits(const char *name, const double *img, int nx, int ny) {
+  FILE *f = fopen(name, "wb");
+  if (!f) return -1;
+  char hdr[2880];
+  memset(hdr, ' ', sizeof(hdr));
+  const char *cards[6];
+  char c[6][81];
+  snprintf(c[0], 81, "%-8s= %20s", "SIMPLE", "T");
+  snprintf(c[1], 81, "%-8s= %20d", "BITPIX", -64);
+  snprintf(c[2], 81, "%-8s= %20d", "NAXIS", 2);
+  snprintf(c[3], 81, "%-8s= %20d", "NAXIS1", nx);
+  snprintf(c[4], 81, "%-8s= %20d", "NAXIS2", ny);
+  snprintf(c[5], 81, "%-8s= %20s", "EXTEND", "T");
+  for (int i = 0; i < 6; i++) {
+    cards[i] = c[i];
+    memcpy(hdr + 80 * i, cards[i], strlen(cards[i]));
+  }
+  memcpy(hdr + 80 * 6, "END", 3);
+  int ok = fwrite(hdr, 1, sizeof(hdr), f) == sizeof(hdr);
+  const uint64_t n = (uint64_t)nx * ny;
+  unsigned char buf[8 * 512];
+  for (uint64_t i = 0; i < n && ok;) {
+    const uint64_t m = (n - i) < 512 ? (n - i) : 512;
+    for (uint64_t k = 0; k < m; k++) {
+      uint64_t b;
+      memcpy(&b, img + i + k, 8);
+      for (int byte = 0; byte < 8; byte++) buf[8 * k + byte] = (unsigned char)(b >> (56 - 8 * byte));
+    }
+    ok = fwrite(buf, 8, m, f) == m;
+    i += m;
+  }
+  const uint64_t used = (8 * n) % 2880;
+  if (ok && used) {
+    memset(hdr, 0, sizeof(hdr));
+    ok = fwrite(hdr, 1, 2880 - used, f) == 2880 - used;
+  }
+  return (fclose(f) == 0 && ok) ? 0 : -1;
 }
 
 static int read_params(const char *fname, params_t *p) {
@@ -98,6 +142,7 @@ static int read_params(const char *fname, params_t *p) {
     else if (!strcmp(k, "precision")) p->precision = !strcmp(v, "mixed") ? RICK_PREC_MIXED : RICK_PREC_FP64;
     else if (!strcmp(k, "phase_on")) p->phase_on = atoi(v) != 0;
     else if (!strcmp(k, "normalize_uvw")) p->normalize_uvw = atoi(v) != 0;
+    else if (!strcmp(k, "fits")) p->fits = atoi(v) != 0;
     else if (!strncmp(k, "Datapath", 8)) {
       const int i = atoi(k + 8);
       if (i >= 1 && i <= MAX_DATASETS) strcpy(p->datapath[i - 1], v);
@@ -226,6 +271,20 @@ int main(int argc, char **argv) {
     fwrite(img_im, 8, plane, fi);
     fclose(fr);
     fclose(fi);
+    if (P.fits) {  /* fourier_transform.c:227-279, main.c:107-108 */
+      /* dataset 0 writes the reference's names; later datasets prefix their index */
+      char fre2[64], fim2[64];
+      if (ids) {
+        snprintf(fre2, sizeof(fre2), "%dparallel_real.fits", ids);
+        snprintf(fim2, sizeof(fim2), "%dparallel_img.fits", ids);
+      } else {
+        snprintf(fre2, sizeof(fre2), "parallel_real.fits");
+        snprintf(fim2, sizeof(fim2), "parallel_img.fits");
+      }
+      if (write_fits(fre2, img_re, P.grid_size_x, P.grid_size_y) ||
+          write_fits(fim2, img_im, P.grid_size_x, P.grid_size_y))
+        shutdown_rick(RICK_ERR_IO, "cannot write the FITS images", __LINE__);
+    }
     t_write += wall() - t0;
     free(uu); free(vv); free(ww); free(wt); free(vr); free(vi); free(img_re); free(img_im);
     printf("*************************************************************\n");
