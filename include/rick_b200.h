@@ -176,6 +176,22 @@ int rick_plan_image_host(rick_plan *plan, uint64_t nrows, const double *uu, cons
 /* Copy the cube out as FP64 interleaved (wstack layout), scaled to the
  * FFTW-normalised values when it has been transformed.  dst may be host or
  * device memory (is_host). Adds into dst when accumulate != 0 (device dst only). */
+/* Streaming ingest: the same imaging as rick_plan_image_host for a dataset whose
+ * samples arrive in slices of rows (read from disk while earlier slices copy
+ * and bin).  begin takes the host arrays of every row's u, v, w and weights
+ * and runs the position pass; samples takes the host vis_real / vis_img of rows
+ * row0 .. row0+nrows-1, in increasing row order, copies them asynchronously
+ * and bins them -- the buffers of one call may be reused once the next call
+ * has returned (pinned buffers make the copies overlap); end grids, transforms
+ * and corrects, and writes the host image (synchronises).  A begin while an
+ * ingest is unfinished abandons it. */
+int rick_plan_ingest_begin(rick_plan *plan, uint64_t nrows, const double *uu, const double *vv,
+                           const double *ww, const float *weight, int row_selection);
+int rick_plan_ingest_samples(rick_plan *plan, uint64_t row0, uint64_t nrows,
+                             const float *vis_real, const float *vis_img);
+int rick_plan_ingest_end(rick_plan *plan, double resolution, double wmin, double wmax,
+                         double *image_real, double *image_imag);
+
 int rick_plan_export_cube(rick_plan *plan, double *dst, int dst_is_host, void *stream);
 /* Load an FP64 interleaved cube (host or device) into the plan, marked as
  * already transformed and normalised (phase_correction's input). */
@@ -323,6 +339,11 @@ int rick_server_wait(rick_server *server, uint64_t ticket, double timeout_ms,
 int rick_server_get_stats(rick_server *server, rick_server_stats *stats);
 /* Finishes every submitted job, then releases the server. */
 int rick_server_destroy(rick_server *server);
+
+/* Page-locked host memory (for the buffers of rick_plan_ingest_samples and
+ * rick_plan_image_host, whose copies then run asynchronously). */
+int rick_host_alloc(void **ptr, uint64_t bytes);
+int rick_host_free(void *ptr);
 
 /* Names of the kernels this library launches, and how many launches it has
  * issued in this process (for launch accounting). */

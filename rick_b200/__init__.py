@@ -135,6 +135,11 @@ def lib():
                                   [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp])
     L.rick_plan_image_host.argtypes = ([_vp, C.c_uint64] + rows7 +
                                        [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp])
+    L.rick_plan_ingest_begin.argtypes = [_vp, C.c_uint64, _vp, _vp, _vp, _vp, C.c_int]
+    L.rick_plan_ingest_samples.argtypes = [_vp, C.c_uint64, C.c_uint64, _vp, _vp]
+    L.rick_plan_ingest_end.argtypes = [_vp, C.c_double, C.c_double, C.c_double, _vp, _vp]
+    L.rick_host_alloc.argtypes = [C.POINTER(_vp), C.c_uint64]
+    L.rick_host_free.argtypes = [_vp]
     L.rick_plan_export_cube.argtypes = [_vp, _vp, C.c_int, _vp]
     L.rick_plan_import_cube.argtypes = [_vp, _vp, C.c_int, _vp]
     L.rick_plan_get_stats.argtypes = [_vp, C.POINTER(PlanStats)]
@@ -166,7 +171,9 @@ def lib():
                "rick_batch_run", "rick_batch_get_tuning", "rick_batch_get_stats",
                "rick_batch_destroy", "rick_batch_kernels_per_run", "rick_server_create",
                "rick_server_submit", "rick_server_wait", "rick_server_get_stats",
-               "rick_server_destroy", "rick_normalize_uvw"]:
+               "rick_server_destroy", "rick_normalize_uvw", "rick_plan_ingest_begin",
+               "rick_plan_ingest_samples", "rick_plan_ingest_end", "rick_host_alloc",
+               "rick_host_free"]:
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L
@@ -349,6 +356,22 @@ class Plan:
         check(lib().rick_plan_image_host(self._h, nrows, *self._rows(rows), selection,
                                          resolution, wmin, wmax, _ptr(image_re), _ptr(image_im)),
               "rick_plan_image_host")
+
+    def ingest(self, nrows, rows, resolution, wmin, wmax, image_re, image_im,
+               selection=ROWS_ALL, slice_rows=65536):
+        """Streaming ingest (rick_plan_ingest_*) of host rows: u, v, w and weights
+        first, then the samples in slices of ``slice_rows`` rows."""
+        uu, vv, ww, wt, vr, vi = rows
+        nv = self.desc.freq_per_chan * self.desc.polarizations
+        check(lib().rick_plan_ingest_begin(self._h, nrows, _ptr(uu), _ptr(vv), _ptr(ww),
+                                           _ptr(wt), selection), "rick_plan_ingest_begin")
+        for r0 in range(0, nrows, slice_rows):
+            n = min(slice_rows, nrows - r0)
+            check(lib().rick_plan_ingest_samples(self._h, r0, n, _ptr(vr) + 4 * r0 * nv,
+                                                 _ptr(vi) + 4 * r0 * nv),
+                  "rick_plan_ingest_samples")
+        check(lib().rick_plan_ingest_end(self._h, resolution, wmin, wmax, _ptr(image_re),
+                                         _ptr(image_im)), "rick_plan_ingest_end")
 
     def export_cube(self, dst, dst_is_host, stream=None):
         check(lib().rick_plan_export_cube(self._h, _ptr(dst), int(dst_is_host), _stream(stream)),

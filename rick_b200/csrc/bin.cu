@@ -337,18 +337,15 @@ void launch_scatter(int blocks, cudaStream_t st, const double *uu, const double 
 
 int lanes_per_row(uint64_t per_row);
 
-int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
-             const double *vv, const double *ww, const float *weight, const float *vis_re,
-             const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
-             uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid) {
-  (void)kernel;
-  (void)precision;
+// Pass 1 and the offsets: histogram of records per bin over all rows, bin
+// offsets and work-item offsets (records are not written yet).
+int bin_count_rows(const Geometry &g, uint64_t nrows, const double *uu, const double *vv,
+                   const double *ww, Scratch &s, uint32_t max_chunk, cudaStream_t st) {
   const uint64_t nbins = g.nbins();
   RICK_CUDA(cudaMemsetAsync(s.bin_count, 0, (nbins + 1) * sizeof(uint32_t), st));
   RICK_CUDA(cudaMemsetAsync(s.bin_cursor, 0, nbins * sizeof(uint32_t), st));
   if (nrows == 0) {
     RICK_CUDA(cudaMemsetAsync(s.item_off, 0, (nbins + 1) * sizeof(uint32_t), st));
-    if (mid) RICK_CUDA(cudaEventRecord(mid, st));
     return RICK_OK;
   }
   const int sms = num_sms();
@@ -365,8 +362,19 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
   k_item_count<<<blocks_items, 256, 0, st>>>(s.bin_count, nbins, max_chunk, s.item_off);
   RICK_CUDA(cudaGetLastError());
   RICK_TRY(exclusive_scan_u32(s.item_off, s.item_off, nbins + 1, s.scan_tmp, st));
-  if (mid) RICK_CUDA(cudaEventRecord(mid, st));
+  return RICK_OK;
+}
 
+// Pass 2 over rows [0, nrows) of the arrays given (a contiguous slice of the
+// rows pass 1 counted: records are placed through the shared bin cursors, so
+// slices may follow one another in any order).
+int bin_scatter_rows(const Geometry &g, uint64_t nrows, const double *uu, const double *vv,
+                     const double *ww, const float *weight, const float *vis_re,
+                     const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
+                     cudaStream_t st) {
+  if (nrows == 0) return RICK_OK;
+  const int sms = num_sms();
+  const uint64_t warps_needed = (nrows + 31) / 32;
   const uint64_t nv = (uint64_t)nchan * npol;
   const bool aligned = ((uintptr_t)vis_re % 16 == 0) && ((uintptr_t)vis_im % 16 == 0);
   const bool v4 = aligned && nv % 4 == 0 && (npol == 1 || npol == 2 || npol == 4);
@@ -394,6 +402,17 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
 #undef RICK_SCATTER
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
+}
+
+int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const double *uu,
+             const double *vv, const double *ww, const float *weight, const float *vis_re,
+             const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
+             uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid) {
+  (void)kernel;
+  (void)precision;
+  RICK_TRY(bin_count_rows(g, nrows, uu, vv, ww, s, max_chunk, st));
+  if (mid) RICK_CUDA(cudaEventRecord(mid, st));
+  return bin_scatter_rows(g, nrows, uu, vv, ww, weight, vis_re, vis_im, nchan, npol, s, st);
 }
 
 // Lanes that share one row's samples: enough to cover the row's loads in one

@@ -216,14 +216,12 @@ int main(int argc, char **argv) {
            (unsigned long long)nm, M.freq_per_chan, M.polarisations,
            (unsigned long long)(nm * nv));
     double *uu = malloc(nm * 8 + 8), *vv = malloc(nm * 8 + 8), *ww = malloc(nm * 8 + 8);
-    float *wt = malloc(nm * npol * 4 + 4), *vr = malloc(nm * nv * 4 + 4), *vi = malloc(nm * nv * 4 + 4);
-    if (!uu || !vv || !ww || !wt || !vr || !vi)
+    float *wt = malloc(nm * npol * 4 + 4);
+    if (!uu || !vv || !ww || !wt)
       shutdown_rick(RICK_ERR_NOT_ENOUGH_MEM, "Not enough memory for the dataset", __LINE__);
     const char *dir = P.datapath[ids];
     if (read_file(dir, P.ufile, uu, nm * 8) || read_file(dir, P.vfile, vv, nm * 8) ||
-        read_file(dir, P.wfile, ww, nm * 8) || read_file(dir, P.weightsfile, wt, nm * npol * 4) ||
-        read_file(dir, P.visrealfile, vr, nm * nv * 4) ||
-        read_file(dir, P.visimgfile, vi, nm * nv * 4))
+        read_file(dir, P.wfile, ww, nm * 8) || read_file(dir, P.weightsfile, wt, nm * npol * 4))
       shutdown_rick(RICK_ERR_IO, "error reading the binMS files", __LINE__);
     t_setup += wall() - t0;
 
@@ -250,9 +248,35 @@ int main(int argc, char **argv) {
     const uint64_t plane = (uint64_t)P.grid_size_x * P.grid_size_y;
     double *img_re = calloc(plane, 8), *img_im = calloc(plane, 8);
     if (!img_re || !img_im) shutdown_rick(RICK_ERR_NOT_ENOUGH_MEM, "image allocation", __LINE__);
-    st = rick_plan_image_host(plan, nm, uu, vv, ww, wt, vr, vi, RICK_ROWS_SECTOR0, resolution,
-                              M.wmin, M.wmax, img_re, img_im);
+    /* the samples stream from disk in slices of rows into two pinned buffer pairs:
+     * a slice is read while the previous one copies and bins */
+    st = rick_plan_ingest_begin(plan, nm, uu, vv, ww, wt, RICK_ROWS_SECTOR0);
     if (st != RICK_OK) shutdown_rick(st, rick_last_error_message(), __LINE__);
+    const uint64_t slice = nv ? (64ull << 20) / (nv * 4) + 1 : 1;
+    void *buf[2][2] = {{NULL, NULL}, {NULL, NULL}};
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 2; c++)
+        if (rick_host_alloc(&buf[b][c], slice * nv * 4 + 16) != RICK_OK)
+          shutdown_rick(RICK_ERR_NOT_ENOUGH_MEM, "pinned sample buffers", __LINE__);
+    char fre_in[NAME_LEN], fim_in[NAME_LEN];
+    if (path_join(fre_in, dir, P.visrealfile) || path_join(fim_in, dir, P.visimgfile))
+      shutdown_rick(RICK_ERR_IO, "binMS path too long", __LINE__);
+    FILE *fr_in = fopen(fre_in, "rb"), *fi_in = fopen(fim_in, "rb");
+    if (!fr_in || !fi_in) shutdown_rick(RICK_ERR_IO, "error opening the visibility files", __LINE__);
+    for (uint64_t r0 = 0, k = 0; r0 < nm; r0 += slice, k++) {
+      const uint64_t n = (nm - r0) < slice ? (nm - r0) : slice;
+      float *a = buf[k & 1][0], *b = buf[k & 1][1];
+      if (fread(a, 4, n * nv, fr_in) != n * nv || fread(b, 4, n * nv, fi_in) != n * nv)
+        shutdown_rick(RICK_ERR_IO, "error reading the binMS files", __LINE__);
+      st = rick_plan_ingest_samples(plan, r0, n, a, b);
+      if (st != RICK_OK) shutdown_rick(st, rick_last_error_message(), __LINE__);
+    }
+    fclose(fr_in);
+    fclose(fi_in);
+    st = rick_plan_ingest_end(plan, resolution, M.wmin, M.wmax, img_re, img_im);
+    if (st != RICK_OK) shutdown_rick(st, rick_last_error_message(), __LINE__);
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 2; c++) rick_host_free(buf[b][c]);
     rick_plan_stats stats;
     rick_plan_get_stats(plan, &stats);
     printf("rows gridded %llu, dropped %llu, records %llu\n",
@@ -286,12 +310,12 @@ int main(int argc, char **argv) {
         shutdown_rick(RICK_ERR_IO, "cannot write the FITS images", __LINE__);
     }
     t_write += wall() - t0;
-    free(uu); free(vv); free(ww); free(wt); free(vr); free(vi); free(img_re); free(img_im);
+    free(uu); free(vv); free(ww); free(wt); free(img_re); free(img_im);
     printf("*************************************************************\n");
   }
   const double total = wall() - t_total;
   printf("%40s time: %g sec\n", "Setup", t_setup);
-  printf("%40s time : %g sec\n", "Imaging (grid+fft+phase)", t_kernel);
+  printf("%40s time : %g sec\n", "Imaging (sample read+grid+fft+phase)", t_kernel);
   printf("%40s time : %g sec\n", "Image writing", t_write);
   printf("%40s time : %g sec\n", "TOT", total);
   FILE *tf = fopen(P.timingfile, "w");

@@ -289,6 +289,26 @@ const char *rick_status_string(int status) {
   }
 }
 
+int rick_host_alloc(void **ptr, uint64_t bytes) {
+  if (!ptr) return set_error(RICK_ERR_INVALID_ARG, "null pointer");
+  *ptr = nullptr;
+  const cudaError_t e = cudaMallocHost(ptr, bytes ? bytes : 1);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver
+                         ? RICK_ERR_NO_ACCELERATORS_FOUND
+                         : RICK_ERR_NOT_ENOUGH_MEM,
+                     "cudaMallocHost of %llu bytes: %s", (unsigned long long)bytes,
+                     cudaGetErrorString(e));
+  }
+  return RICK_OK;
+}
+
+int rick_host_free(void *ptr) {
+  if (ptr) cudaFreeHost(ptr);
+  return RICK_OK;
+}
+
 int rick_kernel_names(const char **names, int max_names) {
   static const char *k[] = {"k_bin_count",        "k_item_count",       "k_bin_scatter",
                             "k_scan_block",       "k_scan_add",         "k_grid_tiles",

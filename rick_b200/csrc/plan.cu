@@ -139,6 +139,14 @@ struct rick_plan {
   double *d_img = nullptr;     // [2*Ny*Nx] image staging for host calls
   double *d_stage = nullptr;   // conversion staging for mixed import/export
   void *d_norm = nullptr;      // NORMALIZE_UVW scratch (extrema)
+  uint32_t chunk = 1024;       // gridder records per work item of the current gridding
+  // streaming ingest (rick_plan_ingest_*): rows staged in h_rows_d, samples by slices
+  bool ingest = false;
+  uint64_t ing_rows = 0, ing_next = 0;
+  int ing_select = 0;
+  cudaStream_t ing_comp = nullptr, ing_copy = nullptr;
+  cudaEvent_t ing_ev[2] = {nullptr, nullptr};
+  int ing_k = 0;
   size_t stage_bytes = 0;
   uint64_t last_rows = 0;
   size_t device_bytes = 0;
@@ -315,15 +323,16 @@ BatchJob plan_job(const rick_plan *p) {
   return j;
 }
 
-int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
-                   const double *ww, const float *weight, const float *vis_re, const float *vis_im,
-                   int select, int accumulate, double dx, double dw, cudaStream_t st,
-                   bool sparse = false) {
+// Gridding in three steps, so that the samples may arrive in slices between the
+// first and the last (rick_plan_ingest_*): the row positions of all rows
+// (normalised if asked, histogram, offsets), the samples of a slice of rows,
+// then the tiles.
+int grid_begin(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+               const double *ww, int select, double dx, double dw, cudaStream_t st) {
   if (nrows > p->d.max_rows)
     return set_error(RICK_ERR_INVALID_ARG, "nrows %llu exceeds the plan capacity %llu",
                      (unsigned long long)nrows, (unsigned long long)p->d.max_rows);
-  if (nrows && (!uu || !vv || !ww || !weight || !vis_re || !vis_im))
-    return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
+  if (nrows && (!uu || !vv || !ww)) return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
   fill_geometry(p, dx, dw, select);
   for (int k = 0; k < RICK_NUM_STAGES; k++) p->ran[k] = false;
   RICK_TRY(mark(p, p->ev[0], st));
@@ -331,10 +340,19 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
     RICK_TRY(normalize_uvw(nrows, const_cast<double *>(uu), const_cast<double *>(vv),
                            const_cast<double *>(ww), p->d_norm, st));
   RICK_CUDA(cudaMemsetAsync(p->s.counters, 0, kNumCounters * sizeof(uint64_t), st));
-  const uint32_t chunk = choose_chunk(nrows);
-  RICK_TRY(bin_rows(p->g, p->d.kernel, p->d.precision, nrows, uu, vv, ww, weight, vis_re, vis_im,
-                    p->d.freq_per_chan, p->d.polarizations, p->s, chunk, st,
-                    p->timing ? p->ev[1] : nullptr));
+  p->chunk = choose_chunk(nrows);
+  RICK_TRY(bin_count_rows(p->g, nrows, uu, vv, ww, p->s, p->chunk, st));
+  return mark(p, p->ev[1], st);
+}
+
+int grid_samples(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+                 const double *ww, const float *weight, const float *vis_re, const float *vis_im,
+                 cudaStream_t st) {
+  return bin_scatter_rows(p->g, nrows, uu, vv, ww, weight, vis_re, vis_im, p->d.freq_per_chan,
+                          p->d.polarizations, p->s, st);
+}
+
+int grid_finish(rick_plan *p, uint64_t nrows, int accumulate, bool sparse, cudaStream_t st) {
   RICK_TRY(mark(p, p->ev[2], st));
   if (sparse) {
     // only the tiles several work items add into are cleared; the row mask
@@ -347,8 +365,8 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
     RICK_CUDA(cudaMemsetAsync(p->cube, 0, p->cube_vals * p->val_bytes, st));
   }
   RICK_TRY(mark(p, p->ev[3], st));
-  RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, chunk, st,
-                      sparse ? p->f.rowmask : nullptr, sparse ? p->f.tilemask : nullptr));
+  RICK_TRY(grid_tiles(p->g, p->d.kernel, p->d.precision, p->s, p->cube, accumulate, p->chunk,
+                      st, sparse ? p->f.rowmask : nullptr, sparse ? p->f.tilemask : nullptr));
   RICK_TRY(mark(p, p->ev[4], st));
   p->ran[0] = p->ran[1] = p->ran[3] = true;
   p->ran[2] = !accumulate;
@@ -357,13 +375,21 @@ int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double 
   return RICK_OK;
 }
 
+int plan_grid_impl(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+                   const double *ww, const float *weight, const float *vis_re, const float *vis_im,
+                   int select, int accumulate, double dx, double dw, cudaStream_t st,
+                   bool sparse = false) {
+  if (nrows && (!weight || !vis_re || !vis_im))
+    return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
+  RICK_TRY(grid_begin(p, nrows, uu, vv, ww, select, dx, dw, st));
+  RICK_TRY(grid_samples(p, nrows, uu, vv, ww, weight, vis_re, vis_im, st));
+  return grid_finish(p, nrows, accumulate, sparse, st);
+}
+
 // grid -> touched-row FFT -> column FFT fused with the w-correction.
-int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
-                      const double *ww, const float *weight, const float *vis_re,
-                      const float *vis_im, int select, double resolution, double wmin,
-                      double wmax, double *img_re, double *img_im, cudaStream_t st) {
-  RICK_TRY(plan_grid_impl(p, nrows, uu, vv, ww, weight, vis_re, vis_im, select, 0,
-                          1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, st, true));
+// The sparse-aware FFT passes and the fused w-correction after a sparse gridding.
+int image_sparse_after_grid(rick_plan *p, uint64_t nrows, double resolution, double wmin,
+                            double wmax, double *img_re, double *img_im, cudaStream_t st) {
   RICK_TRY(mark(p, p->ev_fft0, st));
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y;
   BatchJob j = plan_job(p);
@@ -389,6 +415,15 @@ int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const doub
   p->ran[4] = p->ran[5] = true;
   p->cube_state = kCubeSparse;
   return RICK_OK;
+}
+
+int plan_image_sparse(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+                      const double *ww, const float *weight, const float *vis_re,
+                      const float *vis_im, int select, double resolution, double wmin,
+                      double wmax, double *img_re, double *img_im, cudaStream_t st) {
+  RICK_TRY(plan_grid_impl(p, nrows, uu, vv, ww, weight, vis_re, vis_im, select, 0,
+                          1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, st, true));
+  return image_sparse_after_grid(p, nrows, resolution, wmin, wmax, img_re, img_im, st);
 }
 
 int plan_fft_impl(rick_plan *p, cudaStream_t st) {
@@ -576,6 +611,10 @@ int rick_plan_destroy(rick_plan *p) {
   DeviceGuard guard(p->device);
   cudaDeviceSynchronize();
   if (p->fft) cufftDestroy(p->fft);
+  if (p->ing_comp) cudaStreamDestroy(p->ing_comp);
+  if (p->ing_copy) cudaStreamDestroy(p->ing_copy);
+  for (cudaEvent_t e : p->ing_ev)
+    if (e) cudaEventDestroy(e);
   void *ptrs[] = {p->cube, p->s.bin_count, p->s.bin_cursor, p->s.item_off, p->s.scan_tmp,
                   p->s.counters, p->s.records, p->s.table, p->d_lm, p->fft_work, p->h_rows_d,
                   p->d_img, p->d_stage, p->d_norm, p->f.rowmask, p->f.rowlist, p->f.counts,
@@ -635,6 +674,62 @@ int rick_plan_image(rick_plan *p, uint64_t nrows, const double *uu, const double
                          image_real, image_imag, 0, st);
 }
 
+namespace {
+
+// Device copies of one dataset's rows, in the plan's staging block: uu, vv, ww
+// (doubles) then weights, vis_re, vis_im (floats), each 256-byte aligned.
+struct RowsDev {
+  double *uu, *vv, *ww;
+  float *wt, *vr, *vi;
+};
+
+int stage_rows(rick_plan *p, uint64_t nrows, RowsDev *r) {
+  const uint64_t npol = p->d.polarizations, nv = (uint64_t)p->d.freq_per_chan * npol;
+  auto up = [](uint64_t b) { return (b + 255) & ~255ull; };
+  if (!p->h_rows_d) {
+    const uint64_t cap = p->d.max_rows;
+    const uint64_t cap_bytes = 3 * up(cap * 8) + up(cap * npol * 4) + 2 * up(cap * nv * 4);
+    RICK_TRY(dev_alloc(p, (void **)&p->h_rows_d, cap_bytes));
+    p->rows_cap = cap;
+  }
+  if (!p->d_img) RICK_TRY(dev_alloc(p, (void **)&p->d_img, 16ull * p->d.grid_size_x * p->d.grid_size_y));
+  const uint64_t o_vv = up(nrows * 8), o_ww = o_vv + up(nrows * 8), o_wt = o_ww + up(nrows * 8);
+  const uint64_t o_vr = o_wt + up(nrows * npol * 4), o_vi = o_vr + up(nrows * nv * 4);
+  char *base = (char *)p->h_rows_d;
+  r->uu = (double *)base;
+  r->vv = (double *)(base + o_vv);
+  r->ww = (double *)(base + o_ww);
+  r->wt = (float *)(base + o_wt);
+  r->vr = (float *)(base + o_vr);
+  r->vi = (float *)(base + o_vi);
+  return RICK_OK;
+}
+
+int h2d(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  if (bytes) RICK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  return RICK_OK;
+}
+
+// The gridded plan's image into host arrays (after the gridding on st).
+int image_to_host(rick_plan *p, uint64_t nrows, double resolution, double wmin, double wmax,
+                  double *image_real, double *image_imag, cudaStream_t st) {
+  const uint64_t plane = (uint64_t)p->d.grid_size_x * p->d.grid_size_y;
+  if (p->sparse) {
+    RICK_TRY(image_sparse_after_grid(p, nrows, resolution, wmin, wmax, p->d_img, p->d_img + plane,
+                                     st));
+  } else {
+    RICK_TRY(plan_fft_impl(p, st));
+    RICK_TRY(plan_phase_impl(p, p->d.grid_size_x, p->d.grid_size_y, resolution, wmin, wmax,
+                             p->d_img, p->d_img + plane, 0, st));
+  }
+  RICK_CUDA(cudaMemcpyAsync(image_real, p->d_img, plane * 8, cudaMemcpyDeviceToHost, st));
+  RICK_CUDA(cudaMemcpyAsync(image_imag, p->d_img + plane, plane * 8, cudaMemcpyDeviceToHost, st));
+  RICK_CUDA(cudaStreamSynchronize(st));
+  return RICK_OK;
+}
+
+}  // namespace
+
 int rick_plan_image_host(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
                          const double *ww, const float *weight, const float *vis_real,
                          const float *vis_img, int row_selection, double resolution,
@@ -642,58 +737,106 @@ int rick_plan_image_host(rick_plan *p, uint64_t nrows, const double *uu, const d
   if (!p || !image_real || !image_imag) return set_error(RICK_ERR_INVALID_ARG, "null argument");
   if (nrows > p->d.max_rows)
     return set_error(RICK_ERR_INVALID_ARG, "nrows exceeds the plan capacity");
+  if (nrows && (!uu || !vv || !ww || !weight || !vis_real || !vis_img))
+    return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
   DeviceGuard guard(p->device);
   const uint64_t npol = p->d.polarizations, nv = (uint64_t)p->d.freq_per_chan * npol;
-  // one block: uu,vv,ww (doubles) then weights, vis_re, vis_im (floats), each 256-byte aligned
-  auto up = [](uint64_t b) { return (b + 255) & ~255ull; };
-  const uint64_t o_vv = up(nrows * 8), o_ww = o_vv + up(nrows * 8), o_wt = o_ww + up(nrows * 8);
-  const uint64_t o_vr = o_wt + up(nrows * npol * 4), o_vi = o_vr + up(nrows * nv * 4);
-  const uint64_t total = o_vi + up(nrows * nv * 4);
-  if (nrows > p->rows_cap || !p->h_rows_d) {
-    if (p->h_rows_d) {
-      cudaFree(p->h_rows_d);
-      p->h_rows_d = nullptr;
-    }
-    const uint64_t cap = p->d.max_rows;
-    const uint64_t cap_bytes = 3 * up(cap * 8) + up(cap * npol * 4) + 2 * up(cap * nv * 4);
-    RICK_TRY(dev_alloc(p, (void **)&p->h_rows_d, cap_bytes));
-    p->rows_cap = cap;
-  }
-  if (!p->d_img) RICK_TRY(dev_alloc(p, (void **)&p->d_img, 16ull * p->d.grid_size_x * p->d.grid_size_y));
-  (void)total;
-  char *base = (char *)p->h_rows_d;
-  double *d_uu = (double *)base, *d_vv = (double *)(base + o_vv), *d_ww = (double *)(base + o_ww);
-  float *d_wt = (float *)(base + o_wt), *d_vr = (float *)(base + o_vr), *d_vi = (float *)(base + o_vi);
+  RowsDev r;
+  RICK_TRY(stage_rows(p, nrows, &r));
   cudaStream_t st = 0;
   RICK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   int status = RICK_OK;
-  auto H2D = [&](void *dst, const void *src, size_t bytes) {
-    if (status == RICK_OK && bytes) {
-      cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
-      if (e != cudaSuccess) status = cuda_status(e, "cudaMemcpyAsync(H2D)", __FILE__, __LINE__);
-    }
+  auto run = [&]() -> int {
+    RICK_TRY(h2d(r.uu, uu, nrows * 8, st));
+    RICK_TRY(h2d(r.vv, vv, nrows * 8, st));
+    RICK_TRY(h2d(r.ww, ww, nrows * 8, st));
+    RICK_TRY(h2d(r.wt, weight, nrows * npol * 4, st));
+    RICK_TRY(h2d(r.vr, vis_real, nrows * nv * 4, st));
+    RICK_TRY(h2d(r.vi, vis_img, nrows * nv * 4, st));
+    RICK_TRY(plan_grid_impl(p, nrows, r.uu, r.vv, r.ww, r.wt, r.vr, r.vi,
+                            row_selection == RICK_ROWS_SECTOR0, 0, 1.0 / p->d.grid_size_x,
+                            1.0 / p->d.num_w_planes, st, p->sparse));
+    return image_to_host(p, nrows, resolution, wmin, wmax, image_real, image_imag, st);
   };
-  H2D(d_uu, uu, nrows * 8);
-  H2D(d_vv, vv, nrows * 8);
-  H2D(d_ww, ww, nrows * 8);
-  H2D(d_wt, weight, nrows * npol * 4);
-  H2D(d_vr, vis_real, nrows * nv * 4);
-  H2D(d_vi, vis_img, nrows * nv * 4);
-  const uint64_t plane = (uint64_t)p->d.grid_size_x * p->d.grid_size_y;
-  if (status == RICK_OK)
-    status = rick_plan_image(p, nrows, d_uu, d_vv, d_ww, d_wt, d_vr, d_vi, row_selection,
-                             resolution, wmin, wmax, p->d_img, p->d_img + plane, st);
-  if (status == RICK_OK) {
-    cudaError_t e = cudaMemcpyAsync(image_real, p->d_img, plane * 8, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(image_imag, p->d_img + plane, plane * 8, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) status = cuda_status(e, "image copy-out", __FILE__, __LINE__);
-  } else {
-    cudaStreamSynchronize(st);
-  }
+  status = run();
+  cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   return status;
+}
+
+// ---- streaming ingest ------------------------------------------------------
+int rick_plan_ingest_begin(rick_plan *p, uint64_t nrows, const double *uu, const double *vv,
+                           const double *ww, const float *weight, int row_selection) {
+  if (!p) return set_error(RICK_ERR_INVALID_ARG, "null plan");
+  if (nrows > p->d.max_rows)
+    return set_error(RICK_ERR_INVALID_ARG, "nrows exceeds the plan capacity");
+  if (nrows && (!uu || !vv || !ww || !weight))
+    return set_error(RICK_ERR_INVALID_ARG, "null row pointer");
+  DeviceGuard guard(p->device);
+  if (!p->ing_comp) {
+    RICK_CUDA(cudaStreamCreateWithFlags(&p->ing_comp, cudaStreamNonBlocking));
+    RICK_CUDA(cudaStreamCreateWithFlags(&p->ing_copy, cudaStreamNonBlocking));
+    for (auto &e : p->ing_ev) RICK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // a dataset left unfinished is abandoned
+  RICK_CUDA(cudaStreamSynchronize(p->ing_copy));
+  RICK_CUDA(cudaStreamSynchronize(p->ing_comp));
+  p->ingest = false;
+  RowsDev r;
+  RICK_TRY(stage_rows(p, nrows, &r));
+  const uint64_t npol = p->d.polarizations;
+  RICK_TRY(h2d(r.uu, uu, nrows * 8, p->ing_comp));
+  RICK_TRY(h2d(r.vv, vv, nrows * 8, p->ing_comp));
+  RICK_TRY(h2d(r.ww, ww, nrows * 8, p->ing_comp));
+  RICK_TRY(h2d(r.wt, weight, nrows * npol * 4, p->ing_comp));
+  RICK_TRY(grid_begin(p, nrows, r.uu, r.vv, r.ww, row_selection == RICK_ROWS_SECTOR0,
+                      1.0 / p->d.grid_size_x, 1.0 / p->d.num_w_planes, p->ing_comp));
+  p->ingest = true;
+  p->ing_rows = nrows;
+  p->ing_next = 0;
+  p->ing_k = 0;
+  return RICK_OK;
+}
+
+int rick_plan_ingest_samples(rick_plan *p, uint64_t row0, uint64_t nrows, const float *vis_real,
+                             const float *vis_img) {
+  if (!p) return set_error(RICK_ERR_INVALID_ARG, "null plan");
+  if (!p->ingest) return set_error(RICK_ERR_INVALID_ARG, "no ingest in progress");
+  if (row0 != p->ing_next || row0 + nrows > p->ing_rows)
+    return set_error(RICK_ERR_INVALID_ARG, "samples of rows %llu..%llu: expected the rows from %llu",
+                     (unsigned long long)row0, (unsigned long long)(row0 + nrows),
+                     (unsigned long long)p->ing_next);
+  if (nrows && (!vis_real || !vis_img)) return set_error(RICK_ERR_INVALID_ARG, "null sample pointer");
+  DeviceGuard guard(p->device);
+  RowsDev r;
+  RICK_TRY(stage_rows(p, p->ing_rows, &r));
+  const uint64_t npol = p->d.polarizations, nv = (uint64_t)p->d.freq_per_chan * npol;
+  const int k = p->ing_k & 1;
+  RICK_TRY(h2d(r.vr + row0 * nv, vis_real, nrows * nv * 4, p->ing_copy));
+  RICK_TRY(h2d(r.vi + row0 * nv, vis_img, nrows * nv * 4, p->ing_copy));
+  RICK_CUDA(cudaEventRecord(p->ing_ev[k], p->ing_copy));
+  RICK_CUDA(cudaStreamWaitEvent(p->ing_comp, p->ing_ev[k], 0));
+  RICK_TRY(grid_samples(p, nrows, r.uu + row0, r.vv + row0, r.ww + row0, r.wt + row0 * npol,
+                        r.vr + row0 * nv, r.vi + row0 * nv, p->ing_comp));
+  // the previous slice's host buffers are free once its copy has completed
+  if (p->ing_k > 0) RICK_CUDA(cudaEventSynchronize(p->ing_ev[k ^ 1]));
+  p->ing_next += nrows;
+  p->ing_k++;
+  return RICK_OK;
+}
+
+int rick_plan_ingest_end(rick_plan *p, double resolution, double wmin, double wmax,
+                         double *image_real, double *image_imag) {
+  if (!p || !image_real || !image_imag) return set_error(RICK_ERR_INVALID_ARG, "null argument");
+  if (!p->ingest) return set_error(RICK_ERR_INVALID_ARG, "no ingest in progress");
+  if (p->ing_next != p->ing_rows)
+    return set_error(RICK_ERR_INVALID_ARG, "only %llu of %llu rows have their samples",
+                     (unsigned long long)p->ing_next, (unsigned long long)p->ing_rows);
+  DeviceGuard guard(p->device);
+  p->ingest = false;
+  RICK_TRY(grid_finish(p, p->ing_rows, 0, p->sparse, p->ing_comp));
+  return image_to_host(p, p->ing_rows, resolution, wmin, wmax, image_real, image_imag,
+                       p->ing_comp);
 }
 
 int rick_plan_export_cube(rick_plan *p, double *dst, int dst_is_host, void *stream) {

@@ -184,6 +184,13 @@ int bin_rows(const Geometry &g, int kernel, int precision, uint64_t nrows, const
              const double *vv, const double *ww, const float *weight, const float *vis_re,
              const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
              uint32_t max_chunk, cudaStream_t st, cudaEvent_t mid = nullptr);
+// The two passes of bin_rows, for callers that stream the samples in slices.
+int bin_count_rows(const Geometry &g, uint64_t nrows, const double *uu, const double *vv,
+                   const double *ww, Scratch &s, uint32_t max_chunk, cudaStream_t st);
+int bin_scatter_rows(const Geometry &g, uint64_t nrows, const double *uu, const double *vv,
+                     const double *ww, const float *weight, const float *vis_re,
+                     const float *vis_im, uint32_t nchan, uint32_t npol, Scratch &s,
+                     cudaStream_t st);
 int grid_tiles(const Geometry &g, int kernel, int precision, Scratch &s, void *cube,
                int accumulate, uint32_t max_chunk, cudaStream_t st,
                uint32_t *rowmask = nullptr, uint32_t *tilemask = nullptr);

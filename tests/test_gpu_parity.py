@@ -213,3 +213,43 @@ def test_launch_count_advances():
                     np.ones(1, np.float32), np.ones(1, np.float32))
     gpu_image(rows, 1, 64, 64, 2, 7, "gauss", 1, 1, 1e-3, -1.0, 1.0)
     assert R.launch_count() - before >= 5
+
+
+@pytest.mark.parametrize("slice_rows", [1000, 7919, 1 << 20])
+def test_streaming_ingest_matches_host_call(c1_small, slice_rows):
+    """rick_plan_ingest_*: samples in slices of rows give the image of the
+    one-call host path (which the oracle pins)."""
+    obs = c1_small
+    n = R.rows_read(obs.meta)
+    nx = 512
+    geom = R.Geometry(nx, nx, 8, 7, "kaiser_bessel", "fp64")
+    res = R.resolution_of(obs.meta)
+    host = (np.ascontiguousarray(obs.uu[:n]), np.ascontiguousarray(obs.vv[:n]),
+            np.ascontiguousarray(obs.ww[:n]), np.ascontiguousarray(obs.weights[: n * 2]),
+            np.ascontiguousarray(obs.vis_re[: n * 16]), np.ascontiguousarray(obs.vis_im[: n * 16]))
+    with R.Plan(geom, n, 8, 2, device=0) as plan:
+        re0, im0 = np.zeros(nx * nx), np.zeros(nx * nx)
+        plan.image_host(n, host, res, obs.meta["wmin"], obs.meta["wmax"], re0, im0, R.ROWS_SECTOR0)
+        re, im = np.zeros(nx * nx), np.zeros(nx * nx)
+        plan.ingest(n, host, res, obs.meta["wmin"], obs.meta["wmax"], re, im, R.ROWS_SECTOR0,
+                    slice_rows=slice_rows)
+    assert rel_l2(re, re0) < 1e-13 and rel_l2(im, im0) < 1e-13
+
+
+def test_streaming_ingest_checks_the_row_order(c1_small):
+    obs = c1_small
+    n = 5000
+    geom = R.Geometry(256, 256, 4, 7, "gauss", "fp64")
+    host = (np.ascontiguousarray(obs.uu[:n]), np.ascontiguousarray(obs.vv[:n]),
+            np.ascontiguousarray(obs.ww[:n]), np.ascontiguousarray(obs.weights[: n * 2]),
+            np.ascontiguousarray(obs.vis_re[: n * 16]), np.ascontiguousarray(obs.vis_im[: n * 16]))
+    L = R.lib()
+    with R.Plan(geom, n, 8, 2, device=0) as plan:
+        h = plan._h
+        p = [R._ptr(x) for x in host]
+        R.check(L.rick_plan_ingest_begin(h, n, p[0], p[1], p[2], p[3], R.ROWS_ALL), "begin")
+        assert L.rick_plan_ingest_samples(h, 100, 10, p[4], p[5]) == R.ERR_INVALID_ARG  # skips rows
+        R.check(L.rick_plan_ingest_samples(h, 0, 10, p[4], p[5]), "samples")
+        out = np.zeros(256 * 256)
+        assert L.rick_plan_ingest_end(h, 1e-3, -1.0, 1.0, R._ptr(out), R._ptr(out)) == \
+            R.ERR_INVALID_ARG  # rows 10.. have no samples
