@@ -985,9 +985,11 @@ int sparse_fft_lists(const FftJobs &f, cudaStream_t st) {
   k_row_list<<<std::max(blocks, 1), 256, 0, st>>>(f.jobs, f.njobs, f.mask_base, nwords,
                                                   f.rowmask, f.rowlist, f.counts);
   RICK_CUDA(cudaGetLastError());
-  RICK_LAUNCHED();
-  k_fft_units<<<1, 32, 0, st>>>(f.jobs, f.njobs, f.counts, f.fft_units);
-  RICK_CUDA(cudaGetLastError());
+  if (!f.one) {  // one job's row pass reads its row count directly
+    RICK_LAUNCHED();
+    k_fft_units<<<1, 32, 0, st>>>(f.jobs, f.njobs, f.counts, f.fft_units);
+    RICK_CUDA(cudaGetLastError());
+  }
   return RICK_OK;
 }
 

@@ -135,7 +135,6 @@ struct rick_plan {
   int lm_xtot = -1, lm_ytot = -1;
   // rows staged by the host entry point
   double *h_rows_d = nullptr;  // device copies of uu,vv,ww,weights,vis (one block)
-  uint64_t rows_cap = 0;
   double *d_img = nullptr;     // [2*Ny*Nx] image staging for host calls
   double *d_stage = nullptr;   // conversion staging for mixed import/export
   void *d_norm = nullptr;      // NORMALIZE_UVW scratch (extrema)
@@ -229,9 +228,6 @@ void fill_geometry(rick_plan *p, double dx, double dw, int select) {
   g.select_sector0 = select;
 }
 
-struct FftBytes {
-  size_t work;
-};
 
 int choose_fft(rick_plan *p) {
   const int nx = p->d.grid_size_x, ny = p->d.grid_size_y, nw = plan_planes(&p->d);
@@ -690,7 +686,6 @@ int stage_rows(rick_plan *p, uint64_t nrows, RowsDev *r) {
     const uint64_t cap = p->d.max_rows;
     const uint64_t cap_bytes = 3 * up(cap * 8) + up(cap * npol * 4) + 2 * up(cap * nv * 4);
     RICK_TRY(dev_alloc(p, (void **)&p->h_rows_d, cap_bytes));
-    p->rows_cap = cap;
   }
   if (!p->d_img) RICK_TRY(dev_alloc(p, (void **)&p->d_img, 16ull * p->d.grid_size_x * p->d.grid_size_y));
   const uint64_t o_vv = up(nrows * 8), o_ww = o_vv + up(nrows * 8), o_wt = o_ww + up(nrows * 8);

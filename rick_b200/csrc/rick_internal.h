@@ -75,13 +75,10 @@ struct Scratch {
   uint32_t *bin_count = nullptr;   // [nbins+1] counts, then exclusive offsets
   uint32_t *bin_cursor = nullptr;  // [nbins]
   uint32_t *item_off = nullptr;    // [nbins+1] work-item offsets
-  uint32_t *item_bin = nullptr;    // [max_items]
-  uint32_t *heavy = nullptr;       // [nbins] bins split into several items
   uint32_t *scan_tmp = nullptr;    // block sums for the scans
   uint64_t *counters = nullptr;    // [8] device counters (see Counter)
   RecF64 *records = nullptr;       // [max_records]
   uint64_t max_records = 0;
-  uint64_t max_items = 0;
   double *table = nullptr;         // 1-D kernel table, 5*support doubles
 };
 
@@ -170,8 +167,6 @@ enum Counter : int {
   kCntGridded = 1,    // rows that produced records
   kCntRecords = 2,    // records written
   kCntItemNext = 3,   // persistent gridder work counter
-  kCntHeavy = 4,      // number of heavy bins
-  kCntOverflow = 5,   // records beyond capacity (must stay 0)
   kCntOtherShard = 6, // rows of planes outside the shard
   kNumCounters = 8
 };
