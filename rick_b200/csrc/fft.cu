@@ -356,6 +356,11 @@ template <int LOGN> constexpr int block_threads() {
 // Blocks of 256 threads (lengths up to 2048) are bounded to 128 registers so
 // that two share an SM.
 template <int LOGN> constexpr int min_blocks() { return block_threads<LOGN>() <= 256 ? 2 : 1; }
+// FP32 column passes of one plane in flight fit 80 registers without spills:
+// three 256-thread blocks share an SM (24 warps against 16 to hide latency).
+template <typename T, int LOGN, int PP> constexpr int col_min_blocks() {
+  return sizeof(T) == 4 && PP == 1 && block_threads<LOGN>() <= 256 ? 3 : min_blocks<LOGN>();
+}
 // The row pass holds no per-pixel state: 64 registers a thread, so that 1024
 // threads (4, 2 or 1 blocks) share an SM.
 template <int LOGN> constexpr int row_min_blocks() { return 1024 / block_threads<LOGN>(); }
@@ -578,7 +583,10 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   T acc_re[kVpt], acc_im[kVpt], ph_re[kVpt], ph_im[kVpt];
 #pragma unroll
   for (int q = 0; q < kVpt; q++) acc_re[q] = acc_im[q] = ph_re[q] = ph_im[q] = (T)0;
-  const T norm = (T)J.norm;  // 1/(Nx*Ny): a power of two, exact in FP32
+  // 1/(Nx*Ny), a power of two (exact in FP32): every rounding commutes with
+  // it (away from underflow), so scaling the sums once at the end gives the
+  // bits of scaling each plane's transform, as the reference does
+  const T norm = (T)J.norm;
   int cur[PP], nxt[PP];
   next_set(-1, cur);
   next_set(cur[PP - 1], nxt);
@@ -636,8 +644,7 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
         const int m = t + q * G;
-        const T p = mul_rn(norm, x[pp][q].re);
-        const T qq = mul_rn(norm, x[pp][q].im);
+        const T p = x[pp][q].re, qq = x[pp][q].im;
         if (phase) {
           if (anchor) {
             const double root = root_of(l, m);
@@ -680,8 +687,8 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int m = t + q * G;
-      J.img_re[(uint64_t)m * nx + n] = (double)acc_re[q];
-      J.img_im[(uint64_t)m * nx + n] = (double)acc_im[q];
+      J.img_re[(uint64_t)m * nx + n] = (double)mul_rn(norm, acc_re[q]);
+      J.img_im[(uint64_t)m * nx + n] = (double)mul_rn(norm, acc_im[q]);
     }
   }
   __syncthreads();  // sstep / smask are rewritten for the next column
@@ -689,7 +696,7 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 
 // One job's column pass (the plan): the job as a kernel parameter.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
-__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+__global__ void __launch_bounds__(block_threads<LOGN>(), col_min_blocks<T, LOGN, PP>())
     k_fft_cols_image(ColJob<T> J) {
   constexpr int G = (1 << LOGN) / kVpt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -703,7 +710,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
 // along y): the column groups of the k-th listed job are col_units[k] ..
 // col_units[k+1]-1.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
-__global__ void __launch_bounds__(block_threads<LOGN>(), min_blocks<LOGN>())
+__global__ void __launch_bounds__(block_threads<LOGN>(), col_min_blocks<T, LOGN, PP>())
     k_fft_cols_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
                      int lo, int hi, const uint32_t *__restrict__ col_units,
                      const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts) {

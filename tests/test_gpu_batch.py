@@ -18,6 +18,7 @@ JOBS = [
     (512, 512, 4, "kaiser_bessel", 7, 4, 2, 8000, R.ROWS_ALL),
     (1024, 1024, 1, "gauss", 7, 3, 2, 4000, R.ROWS_ALL),
     (256, 128, 5, "gauss", 5, 2, 1, 0, R.ROWS_ALL),  # no rows: an all-zero image
+    (256, 4096, 10, "kaiser_bessel", 7, 2, 2, 6000, R.ROWS_ALL),  # 4096-point columns
 ]
 
 
