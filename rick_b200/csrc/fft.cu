@@ -316,18 +316,25 @@ __device__ __forceinline__ void stockham_last_pass_pp(typename V2<T>::t *const *
   }
 }
 
-template <typename T, int LOGN, int PP>
+// Passes of the FFT of N = 2^LOGN points: radix-8 passes, the last one of
+// radix 2, 4 or 8.
+template <int LOGN> __host__ __device__ constexpr int fft_passes() { return LOGN / 3 + (LOGN % 3 ? 1 : 0); }
+
+// after(p) runs between the passes (p = 0 .. passes - 2), behind each pass's
+// closing barrier.
+template <typename T, int LOGN, int PP, typename After>
 __device__ __forceinline__ void fft_to_regs_pp(typename V2<T>::t *const *s, int t,
                                                const typename V2<T>::t *__restrict__ tw,
-                                               Cx<T> out[PP][kVpt]) {
+                                               Cx<T> out[PP][kVpt], After after) {
   constexpr int N = 1 << LOGN;
-  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+  constexpr int REM = LOGN % 3;
   constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
-  constexpr int NPASS = P8 + (REM ? 1 : 0);
+  constexpr int NPASS = fft_passes<LOGN>();
   int Ns = 1;
 #pragma unroll
   for (int p = 0; p < NPASS - 1; p++) {
     stockham_pass_pp<T, N, 8, PP>(s, t, Ns, tw);
+    after(p);
     Ns *= 8;
   }
   stockham_last_pass_pp<T, N, LASTR, PP>(s, t, tw, out);
@@ -549,7 +556,9 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   };
   const uint32_t n = base + grp;
   const bool active = n < (uint32_t)nx;
-  auto load_set = [&](int bset, const int set[PP], int slot) {
+  // rows t + q*G, q in [Q0, Q1), of the planes `set` into buffer set `bset`
+  // (q0, q1 are constants once the pass loop is unrolled)
+  auto load_rows = [&](int q0, int q1, int bset, const int set[PP], int slot) {
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
       if (set[pp] >= nw) continue;
@@ -559,6 +568,7 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
       const V *col = J.cube + blocked_index<T>(set[pp], 0, active ? n : 0, nx, ny);
 #pragma unroll
       for (int q = 0; q < kVpt; q++) {
+        if (q < q0 || q >= q1) continue;
         const int k = t + q * G;
         const bool touched = active && ((mask[k >> 5] >> (k & 31)) & 1u);
         if (DB) {
@@ -606,29 +616,42 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   }
   __syncthreads();
   if (DB && cur[0] < nw) {
-    load_set(0, cur, 0);
+    load_rows(0, kVpt, 0, cur, 0);
     cp_async_commit();
   }
+  // With DB the next set's copies are spread over this set's FFT passes (a
+  // share of the rows before each of the first NS passes): issued all at
+  // once, behind the barrier where every warp stands, they fill the
+  // global-load queue while no warp has arithmetic to issue.  Measured at
+  // 4096 points: FP64 (one plane an iteration) is fastest with the copies in
+  // flight by the second pass, FP32 (two planes) with a share before every pass.
+  constexpr int NS = sizeof(T) == 8 ? 2 : fft_passes<LOGN>();
   int bset = 0, it = 0;
   int last_anchor = -kAnchor, prev_iw = -1;
   while (cur[0] < nw) {
     int nn[PP];
     next_set(nxt[PP - 1], nn);  // the set after the next one
     if (DB) {
-      if (nxt[0] < nw) load_set(bset ^ 1, nxt, (it + 1) & 1);
-      cp_async_commit();
-      cp_async_wait<1>();
+      cp_async_wait<0>();  // this set's copies
     } else {
-      load_set(0, cur, it & 1);
+      load_rows(0, kVpt, 0, cur, it & 1);
     }
+    // every copy of this set has landed; every thread is done with the
+    // previous set's buffers and mask slot
     __syncthreads();
     // this set's mask slot is free now: stage the set after next
     stage_masks(it & 1, nn);
     V *bufs[PP];
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) bufs[pp] = sbase + ((DB ? bset : 0) * PP + pp) * LEN;
+    const bool more = DB && nxt[0] < nw;
+    auto load_share = [&](int c) {  // share c of NS of the next set's rows
+      if (more && c < NS) load_rows(c * kVpt / NS, (c + 1) * kVpt / NS, bset ^ 1, nxt, (it + 1) & 1);
+    };
+    load_share(0);
     Cx<T> x[PP][kVpt];
-    fft_to_regs_pp<T, LOGN, PP>(bufs, t, J.tw, x);
+    fft_to_regs_pp<T, LOGN, PP>(bufs, t, J.tw, x, [&](int p) { load_share(p + 1); });
+    if (DB) cp_async_commit();
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
       const int iw = cur[pp];
@@ -673,7 +696,9 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
         }
       }
     }
-    __syncthreads();
+    // single buffer: the next set is copied at the top of the next iteration
+    // (with DB the barrier there, before any copy into this buffer, suffices)
+    if (!DB) __syncthreads();
     if (DB) bset ^= 1;
 #pragma unroll
     for (int pp = 0; pp < PP; pp++) {
