@@ -60,7 +60,7 @@ class ObsConfig:
 
 
 # The imaging workloads.  Array latitudes are not given by the workload
-# descriptions; the values below are typical sites (stated in DESIGN.md).
+# descriptions; the values below are those of typical sites for each array.
 CONFIGS = {
     # Plain FP64 imaging, small: runs on the reference CPU path.
     "c1": ObsConfig("c1", "disc", 40, 3000.0, 45.0, 45.0, 1.0, 10.0, 8, 120e6, 128e6, 2,
