@@ -253,3 +253,63 @@ def test_streaming_ingest_checks_the_row_order(c1_small):
         out = np.zeros(256 * 256)
         assert L.rick_plan_ingest_end(h, 1e-3, -1.0, 1.0, R._ptr(out), R._ptr(out)) == \
             R.ERR_INVALID_ARG  # rows 10.. have no samples
+
+
+@pytest.mark.parametrize("nchan,npol", [(64, 4), (5, 4), (33, 1)])
+def test_wide_rows_match_oracle(nchan, npol):
+    """Rows of many samples (64 x 4 is the LOFAR-like workload's row: the sample
+    pass spreads it over 32 lanes with vector loads; 5 x 4 and 33 x 1 take the
+    16- and 32-lane forms without them), a few NaN samples skipped as the
+    reference skips them (w-stacking.cu:191-192)."""
+    rng = np.random.default_rng(40 + nchan + npol)
+    n, nx, nw = 2500, 256, 6
+    uu = np.clip(0.5 + 0.18 * rng.standard_normal(n), 0, 1)
+    vv = np.clip(0.5 + 0.18 * rng.standard_normal(n), 0, 0.9999)
+    ww = rng.random(n) * 0.999
+    wt = rng.uniform(0.5, 1.5, n * npol).astype(np.float32)
+    vr = rng.standard_normal(n * nchan * npol).astype(np.float32)
+    vi = rng.standard_normal(n * nchan * npol).astype(np.float32)
+    vr[rng.random(vr.size) < 0.01] = np.nan
+    want, dropped = O.wstack("kaiser_bessel", nw, nchan, npol, uu, vv, ww, vr, vi, wt, 1 / nx,
+                             1 / nw, 7, nx, nx)
+    rows = gpu_rows(uu, vv, ww, wt, vr, vi)
+    grid, st = gpu_grid(rows, n, nx, nx, nw, 7, "kaiser_bessel", nchan, npol,
+                        selection=R.ROWS_ALL)
+    assert rel_l2(grid, want) < TOL_FP64
+    assert st["rows_dropped"] == dropped
+    res, wmin, wmax = 1.0 / (2.4 * nx), -140.0, 120.0
+    gss = O.fft_planes(want, nw, nx, nx)
+    want_re, want_im = O.phase_correction(gss, nx, nx, nw, res, wmin, wmax, True)
+    re, im, _ = gpu_image(rows, n, nx, nx, nw, 7, "kaiser_bessel", nchan, npol, res, wmin, wmax,
+                          selection=R.ROWS_ALL)
+    assert rel_l2(re, want_re) < TOL_FP64 and rel_l2(im, want_im) < TOL_FP64
+    re2, im2, _ = gpu_image(rows, n, nx, nx, nw, 7, "kaiser_bessel", nchan, npol, res, wmin,
+                            wmax, selection=R.ROWS_ALL, precision="mixed")
+    err = rel_l2(np.concatenate([re2, im2]), np.concatenate([want_re, want_im]))
+    assert err < TOL_MIXED
+
+
+def test_grid_and_plane_edges_match_oracle():
+    """Rows on the edges: u, v at 0 and 1 and a few cells inside and outside
+    them (footprints clipped by the grid or entirely off it; below -half a
+    support the reference's unsigned bounds would wrap, so those rows are
+    dropped), w on plane boundaries, at 0, just below 0 (truncation toward zero
+    keeps it on plane 0), just below 1 and at 1 (dropped: plane Nw)
+    (w-stacking.cu:143-149)."""
+    nx, nw = 128, 5
+    dx, dw = 1.0 / nx, 1.0 / nw
+    edges = np.array([-4.5 * dx, -2.5 * dx, 0.0, 1e-12, 0.5 * dx, dx, 2.5 * dx, 0.5,
+                      1 - 2.5 * dx, 1 - dx, 1 - 1e-12, 1.0, 1 + 2 * dx, 1 + 5 * dx])
+    wvals = np.array([-1e-12, 0.0, dw, 2 * dw, 0.5, 4 * dw, 1 - 1e-12, 1.0])
+    uu, vv, ww = [a.ravel() for a in np.meshgrid(edges, edges, wvals, indexing="ij")]
+    n = len(uu)
+    rng = np.random.default_rng(77)
+    wt = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    vr = rng.standard_normal(n * 2).astype(np.float32)
+    vi = rng.standard_normal(n * 2).astype(np.float32)
+    for kernel, sup in (("kaiser_bessel", 7), ("gauss_hi", 9)):
+        want, dropped = O.wstack(kernel, nw, 2, 1, uu, vv, ww, vr, vi, wt, dx, dw, sup, nx, nx)
+        grid, st = gpu_grid(gpu_rows(uu, vv, ww, wt, vr, vi), n, nx, nx, nw, sup, kernel, 2, 1,
+                            selection=R.ROWS_ALL)
+        assert rel_l2(grid, want) < TOL_FP64, kernel
+        assert st["rows_dropped"] == dropped > 0, kernel
