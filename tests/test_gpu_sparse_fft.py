@@ -47,6 +47,7 @@ def _oracle_image(host, nx, ny, nw, kernel, sup, nchan, npol, res, wmin, wmax, p
     (1024, 1024, 1, "gauss", 7),    # single plane: plain sum
     (256, 4096, 12, "kaiser_bessel", 7),  # 4096-point columns (64 x 64), anchors + steps
     (4096, 128, 3, "gauss", 7),     # 4096-point rows
+    (128, 8192, 10, "kaiser_bessel", 7),  # 8192-point columns, phase at every plane
 ])
 def test_sparse_path_vs_oracle(nx, ny, nw, kernel, sup):
     n, nchan, npol = 6000, 2, 2
