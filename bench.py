@@ -316,8 +316,27 @@ def run_ours(args):
 
     # ---- e2e through the host C-ABI entry point (pinned host buffers)
     e2e = None
-    if not args.no_e2e and not shard_mode:  # shard mode: device-resident rows only
-        host = [r.cpu().pin_memory() for r in rows]
+    e2e_bytes = sum(int(r.numel() * r.element_size()) for r in rows) + 16 * nx * ny
+    run_e2e = not args.no_e2e and not shard_mode  # shard mode: device-resident rows only
+    if run_e2e and world > 1:
+        # every rank pins its own copy of the inputs: all ranks skip the leg
+        # unless the node's free host memory holds them with room to spare
+        import psutil
+        fits = world * e2e_bytes <= 0.6 * psutil.virtual_memory().available
+        flag = torch.tensor([1 if fits else 0], dtype=torch.int32, device=dev)
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        run_e2e = bool(flag.item())
+        if not run_e2e:
+            e2e = {"value": None, "unit": "vis/s",
+                   "skipped": f"{world} ranks x {e2e_bytes / 1e9:.1f} GB of pinned host buffers "
+                              "exceed 60 % of the free host memory"}
+    if run_e2e:
+        # rows copied straight into pinned buffers (no pageable staging copy)
+        host = []
+        for r in rows:
+            h = torch.empty(r.shape, dtype=r.dtype, pin_memory=True)
+            h.copy_(r)
+            host.append(h)
         h_img = torch.empty(2 * nx * ny, dtype=torch.float64).pin_memory()
         geom = R.Geometry(nx, ny, nw, cfg.w_support, cfg.kernel, "fp64")
         with R.Plan(geom, n, nchan, npol, device=local) as plan:
