@@ -594,11 +594,19 @@ def run_served(args, dev, stream, ctx, big):
             span = time.perf_counter() - t0
             st = srv.stats()
             lat = [r["latency_ms"] for r in res]
+            is_big = [v == big["nvis"] for _, v, _, _ in reqs]
+            lat_small = [x for x, b in zip(lat, is_big) if not b] or [float("nan")]
+            lat_big = [x for x, b in zip(lat, is_big) if b] or [float("nan")]
             vis = sum(v for _, v, _, _ in reqs)
             alone = sum(a for _, _, a, _ in reqs)
             out["rates"].append({
                 "rate_jobs_per_s": rate, "jobs": n_req, "big_jobs": sum(1 for j in reqs if j[1] == big["nvis"]),
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                # the two populations apart: snapshot jobs, and the LOFAR-sized ones
+                "snapshot_p50_ms": float(np.percentile(lat_small, 50)),
+                "snapshot_p99_ms": float(np.percentile(lat_small, 99)),
+                "large_p50_ms": float(np.percentile(lat_big, 50)),
+                "large_max_ms": float(np.max(lat_big)),
                 "sustained_vis_per_s": vis / span,
                 "fp64_alone_vis_per_s": vis / (alone * 1e-3),
                 "served_over_fp64_alone_offered": (vis / span) / (vis / (alone * 1e-3)),
