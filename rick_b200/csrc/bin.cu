@@ -88,16 +88,47 @@ __device__ __forceinline__ void offset_bins(uint32_t bins[4], uint32_t bin_base)
   for (int s = 0; s < 4; s++) bins[s] = bins[s] == kNoBin ? kNoBin : bins[s] + bin_base;
 }
 
+// Per-block cache of record counts: the warps of a block add into a
+// direct-mapped shared table and the block adds the table into the global
+// histogram once at its end, so the bins the uv centre shares across time
+// steps take shared- instead of global-memory atomics.  A slot taken by
+// another bin sends the count straight to the global histogram (counts stay
+// exact either way).
+constexpr int kCountCache = 2048;
+struct CountCache {
+  uint32_t key[kCountCache];
+  uint32_t cnt[kCountCache];
+};
+__device__ __forceinline__ void cache_init(CountCache *c) {
+  for (int i = threadIdx.x; i < kCountCache; i += blockDim.x) {
+    c->key[i] = kNoBin;
+    c->cnt[i] = 0;
+  }
+  __syncthreads();
+}
+__device__ __forceinline__ void cache_add(CountCache *c, uint32_t bin, uint32_t n,
+                                          uint32_t *__restrict__ bin_count) {
+  const uint32_t h = (bin * 2654435761u) >> (32 - 11);  // multiplicative hash, 11 bits
+  const uint32_t k = atomicCAS(&c->key[h], kNoBin, bin);
+  if (k == kNoBin || k == bin) atomicAdd(&c->cnt[h], n);
+  else atomicAdd(&bin_count[bin], n);
+}
+__device__ __forceinline__ void cache_flush(CountCache *c, uint32_t *__restrict__ bin_count) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < kCountCache; i += blockDim.x)
+    if (c->cnt[i]) atomicAdd(&bin_count[c->key[i]], c->cnt[i]);
+}
+
 // Pass 1 over rows base..base+31 (one per lane): histogram of records per bin.
 // Lanes of a warp that hit the same bin combine their increments (the uv
-// centre is dense).  Returns 1 on a lane whose row was dropped; `other` counts
-// rows of other shards.
+// centre is dense), then the block's cache combines the warps'.  Returns 1 on a
+// lane whose row was dropped; `other` counts rows of other shards.
 __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
                                                const double *__restrict__ vv,
                                                const double *__restrict__ ww, uint64_t nrows,
                                                const Geometry &g, uint64_t base,
                                                uint32_t bin_base, uint32_t *__restrict__ bin_count,
-                                               uint32_t &other) {
+                                               uint32_t &other, CountCache *cache) {
   const unsigned lane = lane_id();
   const uint64_t i = base + lane;
   RowPos p;
@@ -115,7 +146,7 @@ __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
   for (int s = 0; s < 4; s++) {
     const unsigned peers = __match_any_sync(kFull, bins[s]);
     const unsigned leader = __ffs(peers) - 1;
-    if (bins[s] != kNoBin && lane == leader) atomicAdd(&bin_count[bins[s]], __popc(peers));
+    if (bins[s] != kNoBin && lane == leader) cache_add(cache, bins[s], __popc(peers), bin_count);
   }
   return dropped;
 }
@@ -134,9 +165,12 @@ __global__ void k_bin_count(const double *__restrict__ uu, const double *__restr
                             uint32_t *__restrict__ bin_count, uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  __shared__ CountCache cache;
+  cache_init(&cache);
   uint32_t dropped = 0, other = 0;
   for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32)
-    dropped += count_rows(uu, vv, ww, nrows, g, base, 0, bin_count, other);
+    dropped += count_rows(uu, vv, ww, nrows, g, base, 0, bin_count, other, &cache);
+  cache_flush(&cache, bin_count);
   add_dropped(dropped, other, counters);
 }
 
@@ -147,14 +181,17 @@ __global__ void k_bin_count_batch(const BatchJob *__restrict__ jobs, int njobs,
                                   uint64_t *__restrict__ counters) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  __shared__ CountCache cache;
+  cache_init(&cache);
   uint32_t dropped = 0, other = 0;
   for (uint64_t u = warp; u < total_units; u += nwarps) {
     const int j = batch_job_of(row_units, njobs, u);
     const BatchJob &J = jobs[j];
     const Geometry g = J.g;
     dropped += count_rows(J.uu, J.vv, J.ww, J.nrows, g, (u - row_units[j]) * 32, J.bin_base,
-                          bin_count, other);
+                          bin_count, other, &cache);
   }
+  cache_flush(&cache, bin_count);
   add_dropped(dropped, other, counters);
 }
 
