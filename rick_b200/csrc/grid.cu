@@ -174,14 +174,20 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
       }
     }
     const double su = hi ? gnorm * wu : wu;
+    // the scale is a power of two: (s * cw) * scale == (s * scale) * cw exactly
+    const double sre_s = q.sre * scale, sim_s = q.sim * scale;
+    // footprint rows e with 0 <= k < ny and y0 <= k < y0 + kTile, k = kb + e
+    const int kb = qgv - g.half;
+    const int e_lo = max(max(-kb, y0 - kb), 0);
+    const int e_hi = min(min(g.ny - kb, y0 + kTile - kb), g.support);
+    const int cell0 = (kb - y0) * kPitch + (j - x0);
     for (int e = 0; e < g.support; e++) {
       const double wve = __shfl_sync(kFull, wv, grp_base + e);
-      const int k = qgv - g.half + e;
-      if (col_ok && k >= 0 && k < g.ny && k >= y0 && k < y0 + kTile) {
+      if (col_ok && e >= e_lo && e < e_hi) {
         const double cw = su * wve;
-        const int cell = (k - y0) * kPitch + (j - x0);
-        fix_put<OutT>(&tile->lo_re[cell], &tile->hi_re[cell], (q.sre * cw) * scale);
-        fix_put<OutT>(&tile->lo_im[cell], &tile->hi_im[cell], (q.sim * cw) * scale);
+        const int cell = cell0 + e * kPitch;
+        fix_put<OutT>(&tile->lo_re[cell], &tile->hi_re[cell], sre_s * cw);
+        fix_put<OutT>(&tile->lo_im[cell], &tile->hi_im[cell], sim_s * cw);
       }
     }
   }
