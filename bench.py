@@ -56,8 +56,8 @@ WORKLOAD_TEXT = {
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that ncu
 # measured for each stage's kernel on this workload at full size (FP64 form, one
 # metric pass; profiles/traffic_c2.md has the command and the read/write split).
-NCU_TRAFFIC = {"bin_count": 126_147_328, "bin_scatter": 10_852_195_840,
-               "grid": 461_239_040, "fft": 2_084_131_840, "phase": 2_413_596_416}
+NCU_TRAFFIC = {"bin_count": 126_126_592, "bin_scatter": 10_851_913_216,
+               "grid": 459_853_312, "fft": 2_083_898_112, "phase": 2_413_688_064}
 # the kernel behind each plan stage on the sparse-aware path (FP64, 4096^2)
 STAGE_KERNELS = {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
                  "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
