@@ -120,9 +120,10 @@ __device__ __forceinline__ void cache_flush(CountCache *c, uint32_t *__restrict_
 }
 
 // Pass 1 over rows base..base+31 (one per lane): histogram of records per bin.
-// Lanes of a warp that hit the same bin combine their increments (the uv
-// centre is dense), then the block's cache combines the warps'.  Returns 1 on a
-// lane whose row was dropped; `other` counts rows of other shards.
+// Every lane adds its row's bins into the block's cache (the uv centre is
+// dense: hot bins are counted in shared memory, not by global atomics; a
+// warp-level match before the cache measured slower).  Returns 1 on a lane
+// whose row was dropped; `other` counts rows of other shards.
 __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
                                                const double *__restrict__ vv,
                                                const double *__restrict__ ww, uint64_t nrows,
@@ -143,11 +144,8 @@ __device__ __forceinline__ uint32_t count_rows(const double *__restrict__ uu,
   footprint_bins(p, g, bins);
   offset_bins(bins, bin_base);
 #pragma unroll
-  for (int s = 0; s < 4; s++) {
-    const unsigned peers = __match_any_sync(kFull, bins[s]);
-    const unsigned leader = __ffs(peers) - 1;
-    if (bins[s] != kNoBin && lane == leader) cache_add(cache, bins[s], __popc(peers), bin_count);
-  }
+  for (int s = 0; s < 4; s++)
+    if (bins[s] != kNoBin) cache_add(cache, bins[s], 1u, bin_count);
   return dropped;
 }
 
