@@ -222,8 +222,11 @@ int rick_plan_stage_ms(rick_plan *plan, float *ms, int n);
  * RICK_ERR_INVALID_ARG (rick_wstack_noalloc_capacity gives the row limit for a
  * geometry).  All calls share that array and it keeps the last call's
  * contents; calls whose GPU work overlaps race on it.  The first call on a
- * device looks up the array's device address, so make it before any stream
- * capture.  Asynchronous on `stream`. */
+ * device sets the device up (looks up the arrays' device addresses and fills
+ * a second static array with the kernel tables of every kernel and support,
+ * synchronously), so make it before any stream capture: a first call on a
+ * capturing stream is refused with RICK_ERR_INVALID_ARG.  Later calls copy
+ * nothing from the host.  Asynchronous on `stream`. */
 int rick_wstack_noalloc(int num_w_planes, uint64_t num_points, uint32_t freq_per_chan,
                         uint32_t polarizations, const double *uu, const double *vv,
                         const double *ww, const float *vis_real, const float *vis_img,

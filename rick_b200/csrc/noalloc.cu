@@ -19,9 +19,12 @@
 //  * every call shares the array and it keeps the last call's contents: each
 //    call clears the parts that must start at zero, and calls whose GPU work
 //    overlaps (different streams, or host threads) race on it;
-//  * the first call on a device looks the array's device address up with
-//    cudaGetSymbolAddress (host code only holds a stand-in for the symbol), so
-//    make that first call before any stream capture.
+//  * the first call on a device sets that device up: it looks the arrays'
+//    device addresses up with cudaGetSymbolAddress (host code only holds a
+//    stand-in for each symbol) and fills the kernel tables of every kernel and
+//    support with one synchronous copy, so make that first call before any
+//    stream capture (a first call on a capturing stream is refused); later
+//    calls copy nothing from the host.
 #include <string.h>
 
 #include <mutex>
@@ -36,27 +39,52 @@ constexpr int kMaxDev = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_mu;
-void *g_scratch_addr[kMaxDev] = {};
+// Kernel tables of the three kernels at every odd support 1..kMaxSupport
+// (w-stacking.cu:35-89), filled once per device when the device is set up.
+constexpr int kTabLen = kIncreasePrecision * kMaxSupport;
+constexpr int kSupports = (kMaxSupport + 1) / 2;
+static __device__ __align__(256) double g_noalloc_tables[3][kSupports][kTabLen];
 
-// Device address of the static scratch on the current device, looked up once.
-int scratch_address(void **out) {
+std::mutex g_mu;
+struct DevArrays {
+  void *scratch;
+  double *tables;
+};
+DevArrays g_dev[kMaxDev] = {};
+
+// Device addresses of the static arrays on the current device; the first call
+// on a device looks them up and fills the tables (synchronously).
+int device_arrays(cudaStream_t st, DevArrays *out) {
   int dev = 0;
   RICK_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDev) return set_error(RICK_ERR_UNSUPPORTED, "device ordinal %d", dev);
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (!g_dev[dev].scratch) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    RICK_CUDA(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+      return set_error(RICK_ERR_INVALID_ARG,
+                       "rick_wstack_noalloc: the first call on a device sets it up and must come "
+                       "before any stream capture");
+    DevArrays a{};
+    cudaError_t e = cudaGetSymbolAddress(&a.scratch, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(scratch)", __FILE__, __LINE__);
-    g_scratch_addr[dev] = p;
+    void *t = nullptr;
+    e = cudaGetSymbolAddress(&t, g_noalloc_tables);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(tables)", __FILE__, __LINE__);
+    a.tables = (double *)t;
+    static double host[3][kSupports][kTabLen];
+    for (int k = 0; k < 3; k++)
+      for (int i = 0; i < kSupports; i++) make_table(k, 2 * i + 1, host[k][i]);
+    RICK_CUDA(cudaMemcpy(a.tables, host, sizeof(host), cudaMemcpyHostToDevice));
+    g_dev[dev] = a;
   }
-  *out = g_scratch_addr[dev];
+  *out = g_dev[dev];
   return RICK_OK;
 }
 
 struct Layout {
-  size_t counters, table, bin_count, bin_cursor, item_off, scan_tmp, records, total;
+  size_t counters, bin_count, bin_cursor, item_off, scan_tmp, records, total;
 };
 
 size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -65,7 +93,6 @@ Layout layout_for(uint64_t nbins, uint64_t nrows) {
   Layout L;
   size_t o = 0;
   L.counters = o;   o += up256(kNumCounters * sizeof(uint64_t));
-  L.table = o;      o += up256(kIncreasePrecision * kMaxSupport * sizeof(double));
   L.bin_count = o;  o += up256((nbins + 1) * 4);
   L.bin_cursor = o; o += up256(nbins * 4);
   L.item_off = o;   o += up256((nbins + 1) * 4);
@@ -86,8 +113,13 @@ int rick_wstack_noalloc_capacity(int num_w_planes, int grid_size_x, int grid_siz
                                  uint64_t *max_rows) {
   if (!max_rows || num_w_planes <= 0 || grid_size_x <= 0 || grid_size_y <= 0)
     return set_error(RICK_ERR_INVALID_ARG, "rick_wstack_noalloc_capacity: bad argument");
-  const uint64_t nbins = (uint64_t)num_w_planes * ((grid_size_x + kTile - 1) / kTile) *
-                         ((grid_size_y + kTile - 1) / kTile);
+  const uint64_t tiles = (uint64_t)((grid_size_x + kTile - 1) / kTile) *
+                        (uint64_t)((grid_size_y + kTile - 1) / kTile);
+  if (tiles >= (1ull << 32) || tiles * (uint64_t)num_w_planes >= (1ull << 32)) {  // < 2^63: no wrap
+    *max_rows = 0;
+    return RICK_OK;
+  }
+  const uint64_t nbins = tiles * (uint64_t)num_w_planes;
   // total(n) = base + up256(4*n*sizeof(RecF64)): the largest n whose padded
   // record block still fits (n + 1 rows do not fit)
   const Layout L = layout_for(nbins, 0);
@@ -125,31 +157,34 @@ int rick_wstack_noalloc(int num_w_planes, uint64_t num_points, uint32_t freq_per
   g.dw = dw;
   g.w_supporth = (double)g.half * (1.0 / (double)g.nx);
   g.select_sector0 = 0;
-  const uint64_t nbins = g.nbins();
+  const uint64_t tiles = (uint64_t)g.ntx * (uint64_t)g.nty;  // < 2^52
+  const uint64_t nbins = tiles < (1ull << 32) ? g.nbins() : ~0ull;
+  // bounds that keep the layout arithmetic below from wrapping: no job with
+  // more rows than the scratch holds records for, bin indices in 32 bits
+  if (num_points > kNoAllocScratchBytes / (4 * sizeof(RecF64)) || nbins >= (1ull << 32))
+    return set_error(RICK_ERR_INVALID_ARG,
+                     "rick_wstack_noalloc: %llu rows / %llu bins exceed the static scratch "
+                     "(%llu bytes)", (unsigned long long)num_points, (unsigned long long)nbins,
+                     (unsigned long long)kNoAllocScratchBytes);
   const Layout L = layout_for(nbins, num_points);
   if (L.total > kNoAllocScratchBytes)
     return set_error(RICK_ERR_INVALID_ARG,
                      "rick_wstack_noalloc: the job needs %llu bytes of scratch but the static "
                      "scratch holds %llu (fewer rows or a smaller grid)",
                      (unsigned long long)L.total, (unsigned long long)kNoAllocScratchBytes);
-  void *base = nullptr;
-  RICK_TRY(scratch_address(&base));
-  char *b = (char *)base;
+  cudaStream_t st = (cudaStream_t)stream;
+  DevArrays arr{};
+  RICK_TRY(device_arrays(st, &arr));
+  char *b = (char *)arr.scratch;
   Scratch s{};
   s.counters = (uint64_t *)(b + L.counters);
-  s.table = (double *)(b + L.table);
+  s.table = arr.tables + ((size_t)kernel * kSupports + (w_support - 1) / 2) * kTabLen;
   s.bin_count = (uint32_t *)(b + L.bin_count);
   s.bin_cursor = (uint32_t *)(b + L.bin_cursor);
   s.item_off = (uint32_t *)(b + L.item_off);
   s.scan_tmp = (uint32_t *)(b + L.scan_tmp);
   s.records = (RecF64 *)(b + L.records);
   s.max_records = 4 * num_points;
-  cudaStream_t st = (cudaStream_t)stream;
-  // the kernel table travels by value through a host array (600 bytes)
-  double tab[kIncreasePrecision * kMaxSupport];
-  make_table(kernel, w_support, tab);
-  RICK_CUDA(cudaMemcpyAsync(s.table, tab, sizeof(double) * kIncreasePrecision * w_support,
-                            cudaMemcpyHostToDevice, st));
   // what must start at zero: the counters (bin counts and cursors are cleared
   // by bin_rows itself), and the caller's cube (overwrite semantics)
   RICK_CUDA(cudaMemsetAsync(s.counters, 0, kNumCounters * sizeof(uint64_t), st));

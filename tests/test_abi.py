@@ -124,3 +124,30 @@ def test_driver_requires_argument():
     exe = os.path.join(ROOT, "rick_b200", "rick_imager")
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 1
+
+
+def test_noalloc_rejects_sizes_that_would_wrap_its_layout():
+    """rick_wstack_noalloc refuses a row count whose record block would not fit
+    the static scratch (2^60 rows would wrap a 64-bit byte count) and a
+    geometry with 2^32 or more bins, before any device call; the capacity of
+    such a geometry is 0 rows."""
+    import ctypes as C
+    L = R.lib()
+    f = L.rick_wstack_noalloc
+    f.argtypes = ([C.c_int, C.c_uint64, C.c_uint32, C.c_uint32] + [C.c_void_p] * 6 +
+                  [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                   C.c_void_p])
+    f.restype = C.c_int
+    buf = np.zeros(16)
+    p = buf.ctypes.data            # never dereferenced: the sizes are refused first
+    st = f(8, 1 << 60, 8, 2, p, p, p, p, p, p, 1 / 512, 1 / 8, 7, R.KERNELS["kaiser_bessel"],
+           512, 512, p, None)
+    assert st == R.ERR_INVALID_ARG and "exceed" in R.last_error()
+    st = f(1 << 30, 10, 8, 2, p, p, p, p, p, p, 1 / 65536, 1 / (1 << 30), 7,
+           R.KERNELS["kaiser_bessel"], 1 << 16, 1 << 16, p, None)
+    assert st == R.ERR_INVALID_ARG
+    cap = L.rick_wstack_noalloc_capacity
+    cap.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+    cap.restype = C.c_int
+    rows = C.c_uint64(7)
+    assert cap(1 << 30, 1 << 30, 1 << 30, C.byref(rows)) == R.OK and rows.value == 0
