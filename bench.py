@@ -53,15 +53,24 @@ WORKLOAD_TEXT = {
           "high-precision Gaussian support 9",
 }
 
-# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that ncu
-# measured for each stage's kernel on this workload at full size (FP64 form, one
-# metric pass; profiles/traffic_c2.md has the command and the read/write split).
-NCU_TRAFFIC = {"bin_count": 126_126_592, "bin_scatter": 10_851_913_216,
-               "grid": 459_853_312, "fft": 2_083_898_112, "phase": 2_413_688_064}
-# the kernel behind each plan stage on the sparse-aware path (FP64, 4096^2)
-STAGE_KERNELS = {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
-                 "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
-                 "fft": "k_fft_rows<double,12>", "phase": "k_fft_cols_image<double,12,1,1,1>"}
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
+# captures of a kernel on a workload at full size, keyed by (workload, kernel);
+# each entry names the capture.  A kernel without a capture reports null.
+NCU_TRAFFIC = {
+    ("c2", "k_bin_scatter<32,1>"): (10_851_913_216, "profiles/traffic_c2.md"),
+    ("c2", "k_grid_tiles<double,8>"): (459_853_312, "profiles/traffic_c2.md"),
+    ("c2", "k_fft_rows<double,12>"): (2_083_898_112, "profiles/traffic_c2.md"),
+}
+
+
+def plan_kernel_name(stage, nx, ny):
+    """The kernel behind a plan stage on the sparse-aware path (FP64)."""
+    ly = max(int(ny).bit_length() - 1, 0)
+    lx = max(int(nx).bit_length() - 1, 0)
+    return {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
+            "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
+            "fft": f"k_fft_rows<double,{lx}>",
+            "phase": f"k_fft_cols_image<double,{ly}>"}.get(stage, stage)
 
 
 def fp64_gemm_tflops(dev) -> float:
@@ -303,7 +312,7 @@ def run_ours(args):
         err_mixed_maxabs = float((imgmx - img64).abs().max() / img64.abs().max())
         planmx.close()
     else:
-        msmx, stagemx, latmx, err_mixed = float("nan"), {}, [float("nan")], None
+        msmx, stagemx, latmx, err_mixed, imgmx = float("nan"), {}, [float("nan")], None, None
         err_mixed_maxabs = None
 
     # max over ranks
@@ -330,6 +339,7 @@ def run_ours(args):
             e2e = {"value": None, "unit": "vis/s",
                    "skipped": f"{world} ranks x {e2e_bytes / 1e9:.1f} GB of pinned host buffers "
                               "exceed 60 % of the free host memory"}
+    host = None
     if run_e2e:
         # rows copied straight into pinned buffers (no pageable staging copy)
         host = []
@@ -359,17 +369,20 @@ def run_ours(args):
         e2e = {"value": world * nvis / e2e_s, "unit": "vis/s", "h2d_bytes_per_step": bi,
                "d2h_bytes_per_step": int(h_img.numel() * 8), "steps": k_e2e,
                "ms_per_step": e2e_s * 1e3}
-        del host
 
     hbm, peak_kind = peaks()
     alg = algorithmic_bytes(n, nvis, npol, stats64["records"], nx, ny, nw, 8,
                             stats64.get("fft_rows", 0))
     dom = max(stage64, key=stage64.get)
     achieved = alg[dom] / (stage64[dom] * 1e-3) / 1e9
-    roofline = {"kernel": dom, "kernel_name": STAGE_KERNELS.get(dom, dom),
+    kname = plan_kernel_name(dom, nx, ny)
+    traffic = NCU_TRAFFIC.get((args.workload, kname)) if not args.time_fraction < 1 else None
+    roofline = {"kernel": dom, "kernel_name": kname,
                 "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "traffic": NCU_TRAFFIC.get(dom) if args.workload == "c2" else None,
+                "traffic": traffic[0] if traffic else None,
+                "traffic_source": traffic[1] if traffic else
+                ("no ncu capture of this kernel on this workload"),
                 "peak_source": peak_kind,
                 "algorithmic_bytes": alg[dom],
                 "stages_ms": {k: round(v, 4) for k, v in stage64.items()},
@@ -378,7 +391,8 @@ def run_ours(args):
                 "fft_rows": stats64.get("fft_rows", 0)}
     if dom == "phase" and stats64.get("fft_rows", 0):
         roofline["note"] = ("column FFT + w-correction + plane sum: bound by FP64 issue and "
-                            "latency (one 4096-point column of 16 warps per SM), not by HBM")
+                            "shared-memory traffic, not by HBM (fp64_compute gives the compute "
+                            "roofline)")
         # algorithmic FP64 flops of the column pass: a radix-2-equivalent 5 N log2 N per
         # column FFT of every plane (all planes hold data here), plus the w-correction's
         # ~10 flops per pixel and plane
@@ -395,27 +409,40 @@ def run_ours(args):
                                                    "(torch.matmul float64), best of 5"}
     g8 = 2 * nw * nx * ny * 8
     in_bytes = sum(int(r.numel() * r.element_size()) for r in rows)
-    pipe_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny
-    cpu = None
+    dense_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny
+    sparse_bytes = sum(alg[k] for k in stage64 if k in alg)
+    cpu, oracle_err = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(obs, n, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, steps=1)
+        hrows = _host_rows(host if host is not None else rows)
+        cpu, ref_img = cpu_baseline(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax)
+        del hrows
+        ref_t = torch.from_numpy(ref_img).to(dev)
+        oracle_err = {"oracle": f"the image of the cpu_baseline run ({cpu['kind']} CPU path, "
+                                "FP64, in w-plane chunks)"}
+        for nm, im in (("fp64", img64), ("mixed", imgmx)):
+            if im is None:
+                continue
+            oracle_err[nm] = {
+                "rel_l2": float(torch.linalg.vector_norm(im - ref_t) / torch.linalg.vector_norm(ref_t)),
+                "max_abs_rel_to_peak": float((im - ref_t).abs().max() / ref_t.abs().max())}
+        del ref_t
+    del host
     line = {
         "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
         "scaling": "strong" if shard_mode else "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD_TEXT[args.workload],
-                   "rows": n, "visibilities": nvis, "grid": nx, "w_planes": nw,
-                   "kernel": cfg.kernel, "w_support": cfg.w_support,
-                   "l2": f"inputs ({in_bytes / 1e9:.2f} GB) larger than L2; no flush"
-                         if in_bytes > 126e6 else "inputs smaller than L2",
-                   "parallelism": (f"w-plane shards x{world} + NCCL image all-reduce" if shard_mode
-                                   else f"replicas x{world}"),
-                   "time_fraction": args.time_fraction},
+        "config": config_of(args, cfg, n, nvis, nx, nw, in_bytes, world, shard_mode),
         "e2e": e2e, "gpu_launches": launches,
         "roofline": roofline,
-        "pipeline_roofline": {"bytes": pipe_bytes, "achieved_gbs": pipe_bytes / (ms64 * 1e-3) / 1e9,
-                              "frac": pipe_bytes / (ms64 * 1e-3) / 1e9 / hbm},
+        "pipeline_roofline": {
+            "dense_bytes": dense_bytes,
+            "dense_frac": dense_bytes / (ms64 * 1e-3) / 1e9 / hbm,
+            "dense_note": "the dense algorithm's bytes (a full cube written, FFT-read and "
+                          "-written, read by the w-correction): the bar the path is held to",
+            "moved_bytes": sparse_bytes,
+            "moved_frac": sparse_bytes / (ms64 * 1e-3) / 1e9 / hbm,
+            "moved_note": "the bytes the sparse-aware path itself must move (touched rows only)"},
         "forms": {"fp64": {"vis_per_s": jobs_done * nvis / (ms64 * 1e-3), "ms": ms64,
                            "stages_ms": stage64,
                            "p50_ms": float(np.percentile(lat64, 50)),
@@ -427,7 +454,8 @@ def run_ours(args):
                       "p99_ms": float(np.percentile(latmx, 99)),
                       "rel_l2_vs_fp64": err_mixed,
                       "max_abs_vs_fp64_rel_to_peak": err_mixed_maxabs},
-                  "mixed_over_fp64": (ms64 / msmx) if "mixed" in forms else None},
+                  "mixed_over_fp64": (ms64 / msmx) if "mixed" in forms else None,
+                  "vs_oracle": oracle_err},
         "job": {"rows_gridded": stats64["rows_gridded"], "rows_dropped": stats64["rows_dropped"],
                 "records": stats64["records"], "work_items": stats64["work_items"],
                 "generate_s": gen_s},
@@ -624,104 +652,192 @@ def _threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline(obs, n, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, steps=1,
-                 target_s=6.0):
-    """The reference's CPU path on a bounded sample, extrapolated to the job.
+class CpuJob:
+    """The reference's CPU path for one imaging job, timed in w-plane chunks.
 
-    wstack: the reference's own compiled CPU wstack (oracle/_ref, OpenMP, all host
-    threads) on the first S packed rows, scaled by rows/S; FFT: scipy.fft.ifft2 FP64
-    (workers = all threads; FFTW is absent) on P planes, scaled by Nw/P;
-    phase_correction: the reference's own on P planes, scaled by Nw/P.
-    Falls back to the oracle restatement ("port") where oracle/_ref is absent."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    import torch
+    A chunk is `chunk_planes` consecutive w-planes of the job.  Its step runs,
+    on every host thread: the cube's zeroing, the reference's own compiled CPU
+    ``wstack`` (oracle/_ref, OpenMP) once per plane on that plane's packed rows
+    with Nw' = 1 and w' = 0 (w enters wstack only through grid_w,
+    w-stacking.cu:466-469, so the plane's cells receive exactly the additions
+    of the whole-cube call), the per-plane inverse FFT (scipy.fft, FP64,
+    workers = all threads; FFTW is absent) and the reference's own
+    ``phase_correction`` over the chunk's planes (wmin/wmax shifted to the
+    chunk, the chunk image rescaled by planes/Nw after the step; its 32-bit
+    cube index stays below 2^32 for chunks of <= 8 planes of 8192^2).  Row
+    selection (one rank's sector 0 after the 1000-row drop) and the packing
+    of each plane's rows are set-up outside the timed steps, as the
+    reference's own kernel timer leaves out its sector packing
+    (gridding_cpu.c:88-138).  Steps cycle through the chunks; the job is every
+    chunk once.  Falls back to the oracle's restatement ("port") where
+    oracle/_ref was not built."""
 
-    threads = _threads()
-    kind = "reference" if O.ref_available(cfg.kernel) else "port"
-    nv = nchan * npol
+    def __init__(self, host, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, threads,
+                 chunk_planes=8):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        self.O = O
+        self.kind = "reference" if O.ref_available(cfg.kernel) else "port"
+        self.threads = threads
+        self.nchan, self.npol, self.nx, self.ny, self.nw = nchan, npol, nx, ny, nw
+        self.cfg, self.res, self.wmin, self.wmax = cfg, res, wmin, wmax
+        self.c = max(1, min(chunk_planes, nw))
+        nv = nchan * npol
+        uu, vv, ww, wt, vr, vi = host
+        rows = O.sector0_rows(vv, len(uu) + 1000, nx, ny, cfg.w_support).astype(np.int64)
+        gw = O.plane_of(ww[rows], nw)
+        order = rows[np.argsort(gw, kind="stable")]
+        gws = np.sort(gw, kind="stable")
+        bounds = np.searchsorted(gws, np.arange(nw + 1))
+        self.planes = []
+        for iw in range(nw):
+            r = order[bounds[iw]:bounds[iw + 1]]
+            self.planes.append((np.ascontiguousarray(uu[r]), np.ascontiguousarray(vv[r]),
+                                np.zeros(len(r)),
+                                np.ascontiguousarray(wt.reshape(-1, npol)[r].ravel()),
+                                np.ascontiguousarray(vr.reshape(-1, nv)[r].ravel()),
+                                np.ascontiguousarray(vi.reshape(-1, nv)[r].ravel())))
+        self.nchunks = (nw + self.c - 1) // self.c
+        self.cube = np.zeros(2 * self.c * nx * ny)
+        self.image_re, self.image_im = np.zeros(nx * ny), np.zeros(nx * ny)
+        self.done = [False] * self.nchunks
 
-    def host(x, count):
-        return np.ascontiguousarray(x[:count].cpu().numpy() if hasattr(x, "cpu") else x[:count])
+    def chunk_vis(self, k):
+        a = k * self.c
+        return sum(len(p[0]) for p in self.planes[a:a + self.c]) * self.nchan * self.npol
 
-    # a first small sample sizes the real one to about target_s of wstack
-    def time_wstack(S):
-        uu, vv, ww = host(obs.uu, S), host(obs.vv, S), host(obs.ww, S)
-        wt, vr, vi = host(obs.weights, S * npol), host(obs.vis_re, S * nv), host(obs.vis_im, S * nv)
-        keep = (ww * nw).astype(np.int64) < nw
-        uu, vv, ww = uu[keep], vv[keep], ww[keep]
-        wt = wt.reshape(-1, npol)[keep].ravel(); vr = vr.reshape(-1, nv)[keep].ravel()
-        vi = vi.reshape(-1, nv)[keep].ravel()
-        plane_grid = np.zeros(2 * nw * nx * ny)
-        t0 = time.perf_counter()
-        if kind == "reference":
-            O.ref_lib(cfg.kernel).wstack(nw, len(uu), nchan, npol, uu, vv, ww, vr, vi, wt, 1 / nx,
-                                        1 / nw, cfg.w_support, nx, ny, plane_grid, threads, 0)
-        else:
-            O.wstack(cfg.kernel, nw, nchan, npol, uu, vv, ww, vr, vi, wt, 1 / nx, 1 / nw,
-                     cfg.w_support, nx, ny, plane_grid, threads)
-        return time.perf_counter() - t0, plane_grid
+    def job_vis(self):
+        return sum(self.chunk_vis(k) for k in range(self.nchunks))
 
-    S0 = min(n, 20000)
-    t_small, _ = time_wstack(S0)
-    S = int(min(n, max(S0, S0 * target_s / max(t_small, 1e-3))))
-    results = []
-    for _ in range(steps):
-        t_w, grid = time_wstack(S)
-        P = 2
-        sub = np.ascontiguousarray(grid[: 2 * P * nx * ny])
-        t0 = time.perf_counter()
-        gss = O.fft_planes(sub, P, nx, ny, workers=threads)
-        t_f = time.perf_counter() - t0
+    def step(self, k):
+        """Chunk k end to end; returns its wall-clock seconds."""
+        O, nx, ny, nw = self.O, self.nx, self.ny, self.nw
+        a = k * self.c
+        c = min(self.c, nw - a)
+        cube = self.cube[: 2 * c * nx * ny]
+        dx, dw = 1.0 / nx, 1.0 / nw
+        sup, kern = self.cfg.w_support, self.cfg.kernel
+        dw_ph = (self.wmax - self.wmin) / nw
+        wmin_c = self.wmin + a * dw_ph
         img_re, img_im = np.zeros(nx * ny), np.zeros(nx * ny)
         t0 = time.perf_counter()
-        if kind == "reference":
-            O.ref_lib(cfg.kernel).phase_correction(gss, img_re, img_im, nx, ny, P, nx, ny, res,
-                                                  wmin, wmax, threads, 0)
+        cube.fill(0.0)
+        for p in range(c):
+            uu, vv, ww, wt, vr, vi = self.planes[a + p]
+            plane = cube[2 * p * nx * ny: 2 * (p + 1) * nx * ny]
+            if self.kind == "reference":
+                O.ref_lib(kern).wstack(1, len(uu), self.nchan, self.npol, uu, vv, ww, vr, vi, wt,
+                                       dx, dw, sup, nx, ny, plane, self.threads, 0)
+            else:
+                O.wstack(kern, 1, self.nchan, self.npol, uu, vv, ww, vr, vi, wt, dx, dw, sup, nx,
+                         ny, grid=plane, threads=self.threads)
+        gss = O.fft_planes(cube, c, nx, ny, workers=self.threads)
+        if self.kind == "reference":
+            O.ref_lib(kern).phase_correction(gss, img_re, img_im, nx, ny, c, nx, ny, self.res,
+                                             wmin_c, wmin_c + c * dw_ph, self.threads, 0)
         else:
-            O.phase_correction(gss, nx, ny, P, res, wmin, wmax, True, threads, img_re, img_im)
-        t_p = time.perf_counter() - t0
-        est = t_w * (n / S) + (t_f + t_p) * (nw / P)
-        results.append(dict(est=est, t_w=t_w, t_f=t_f, t_p=t_p))
-    est = float(np.median([r["est"] for r in results]))
-    r0 = results[0]
-    del torch
-    return {"value": n * nv / est, "unit": "vis/s", "cores": threads, "kind": kind,
-            "sample": f"wstack on {S} of {n} rows (x{n / S:.1f}), FFT (scipy.fft, FFTW absent) "
-                      f"and phase_correction on 2 of {nw} planes (x{nw / 2:.0f}); "
-                      f"sample times wstack {r0['t_w']:.2f}s fft {r0['t_f']:.2f}s "
-                      f"phase {r0['t_p']:.2f}s",
-            "est_job_s": est}
+            O.phase_correction(gss, nx, ny, c, self.res, wmin_c, wmin_c + c * dw_ph, True,
+                               self.threads, img_re, img_im)
+        t = time.perf_counter() - t0
+        if not self.done[k]:   # the job's image: each chunk once, at the whole cube's dwnorm
+            self.image_re += img_re * (c / nw)
+            self.image_im += img_im * (c / nw)
+            self.done[k] = True
+        return t
+
+    def describe(self):
+        return (f"the whole job in {self.nchunks} w-plane chunk(s) of {self.c} plane(s) "
+                f"({self.job_vis()} visibilities): the reference's own CPU wstack per plane, "
+                f"scipy.fft FP64 (FFTW absent), the reference's own phase_correction per chunk; "
+                f"{self.threads} OpenMP threads; row selection and packing untimed")
+
+
+def _host_rows(rows):
+    """numpy views (or copies) of the six row arrays on the host."""
+    out = []
+    for r in rows:
+        if hasattr(r, "is_pinned") and r.device.type == "cpu":
+            out.append(r.numpy())
+        elif hasattr(r, "cpu"):
+            out.append(r.cpu().numpy())
+        else:
+            out.append(np.asarray(r))
+    return out
+
+
+def cpu_baseline(host, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax):
+    """The whole job once through CpuJob (every chunk), timed: about 10-30 s of
+    CPU work at the LOFAR-like size.  Returns the cpu_baseline object and the
+    job's image (the reference's own CPU result for the error figures)."""
+    threads = _threads()
+    job = CpuJob(host, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, threads)
+    t = sum(job.step(k) for k in range(job.nchunks))
+    vis = job.job_vis()
+    return ({"value": vis / t, "unit": "vis/s", "cores": threads, "kind": job.kind,
+             "sample": job.describe(), "job_s": t},
+            np.concatenate([job.image_re, job.image_im]))
+
+
+def config_of(args, cfg, n, nvis, nx, nw, in_bytes, world, shard_mode=False):
+    """The workload description both arms print (the same dict)."""
+    return {"workload": WORKLOAD_TEXT[args.workload], "rows": n, "visibilities": nvis,
+            "grid": nx, "w_planes": nw, "kernel": cfg.kernel, "w_support": cfg.w_support,
+            "l2": (f"inputs ({in_bytes / 1e9:.2f} GB) larger than L2; no flush"
+                   if in_bytes > 126e6 else "inputs smaller than L2"),
+            "parallelism": (f"w-plane shards x{world} + NCCL image all-reduce" if shard_mode
+                            else f"replicas x{world}"),
+            "time_fraction": args.time_fraction}
 
 
 def run_reference(args):
-    """Reference arm: the reference's own CPU path, rank 0 only."""
+    """Reference arm: the reference's own CPU path (CpuJob), rank 0 only.  Each
+    step is one w-plane chunk of the job (steps cycle through the chunks, so K
+    steps cover K/chunks whole jobs); W warm-up steps run the same way,
+    untimed; value = visibilities of the timed steps / their summed time."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import rick_b200  # noqa: F401  (synthetic generator only)
-    from rick_b200 import synth
     import torch
+    import rick_b200 as R
+    from rick_b200 import synth
 
     cfg = synth.CONFIGS[args.workload]
     dev = "cuda" if torch.cuda.is_available() else "cpu"
     obs = synth.make_observation(cfg, seed=2024, device=dev, time_fraction=args.time_fraction)
-    import rick_b200 as R
     n = R.rows_read(obs.meta)
     nv = cfg.nchan * cfg.npol
-    res = R.resolution_of(obs.meta)
+    host = _host_rows((obs.uu[:n], obs.vv[:n], obs.ww[:n], obs.weights[: n * cfg.npol],
+                       obs.vis_re[: n * nv], obs.vis_im[: n * nv]))
+    meta = obs.meta
+    del obs
+    nx = args.grid or cfg.grid
+    nw = args.w_planes or cfg.w_planes
+    threads = _threads()
+    job = CpuJob(host, cfg.nchan, cfg.npol, nx, nx, nw, cfg, R.resolution_of(meta),
+                 meta["wmin"], meta["wmax"], threads)
+    in_bytes = sum(int(h.nbytes) for h in host)
+    del host
+    k = 0
     for _ in range(args.warmup):
-        pass  # the sample sizing inside cpu_baseline warms the caches
-    cpu = cpu_baseline(obs, n, cfg.nchan, cfg.npol, cfg.grid, cfg.grid, cfg.w_planes, cfg, res,
-                       obs.meta["wmin"], obs.meta["wmax"], steps=max(1, min(args.steps, 3)))
-    line = {"metric": METRIC, "value": cpu["value"], "unit": "vis/s", "impl": "reference",
+        job.step(k % job.nchunks)
+        k += 1
+    t, vis = 0.0, 0
+    for _ in range(args.steps):
+        t += job.step(k % job.nchunks)
+        vis += job.chunk_vis(k % job.nchunks)
+        k += 1
+    value = vis / t
+    line = {"metric": METRIC, "value": value, "unit": "vis/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": cpu["est_job_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_TEXT[args.workload],
-                       "rows": n, "visibilities": n * nv},
-            "cpu_baseline": cpu,
-            "e2e": {"value": cpu["value"], "unit": "vis/s", "h2d_bytes_per_step": 0,
+            "config": config_of(args, cfg, n, n * nv, nx, nw, in_bytes, world),
+            "cpu_baseline": {"value": value, "unit": "vis/s", "cores": threads, "kind": job.kind,
+                             "sample": f"{args.steps} steps of one w-plane chunk each "
+                                       f"({vis / (job.job_vis() or 1):.2f} jobs); "
+                                       + job.describe()},
+            "e2e": {"value": value, "unit": "vis/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

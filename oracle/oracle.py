@@ -51,6 +51,11 @@ def lib():
                                               C.c_int, C.c_double, C.c_double, C.c_double,
                                               C.c_int, C.c_int]
         L.oracle_phase_correction.restype = C.c_int
+        L.oracle_phase_correction_planes.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int,
+                                                     C.c_int, C.c_int, C.c_int, C.c_int,
+                                                     C.c_double, C.c_double, C.c_double,
+                                                     C.c_int, C.c_int]
+        L.oracle_phase_correction_planes.restype = C.c_int
         L.oracle_sector0_rows.argtypes = [_dp, C.c_uint64, C.c_int, C.c_int, C.c_int, _u64p]
         L.oracle_sector0_rows.restype = C.c_uint64
         L.oracle_normalize_uvw.argtypes = [C.c_uint64, _dp, _dp, _dp, _dp]
@@ -134,6 +139,25 @@ def phase_correction(gridss, nx, ny, nw, resolution, wmin, wmax, phase_on=True, 
     return image_re, image_im
 
 
+def phase_correction_planes(gridss, nx, ny, nw, w_first, w_count, resolution, wmin, wmax,
+                            image_re, image_im, phase_on=True, threads=0):
+    """phase_correction.cu:185-250 over planes w_first..w_first+w_count-1 of an
+    nw-plane cube (``gridss`` holds only those planes), accumulating into the
+    image; consecutive ranges give the bits of one whole-cube call."""
+    rc = lib().oracle_phase_correction_planes(_c(gridss, np.float64), image_re, image_im, nx, ny,
+                                              nw, w_first, w_count, nx, ny, resolution, wmin,
+                                              wmax, int(phase_on), threads)
+    assert rc == 0
+    return image_re, image_im
+
+
+def plane_of(ww, nw):
+    """w-stacking.cu:466-469: grid_w = (int)(ww / dw), dw = 1/Nw (init.c:12):
+    FP64 division, truncation toward zero."""
+    dw = 1.0 / nw
+    return np.trunc(np.asarray(ww, dtype=np.float64) / dw).astype(np.int64)
+
+
 def sector0_rows(vv, nmeasures_file, nx, ny, w_support):
     out = np.zeros(max(int(nmeasures_file), 1), dtype=np.uint64)
     n = lib().oracle_sector0_rows(_c(vv, np.float64), nmeasures_file, nx, ny, w_support, out)
@@ -172,6 +196,47 @@ def image(obs, nx, ny, nw, kernel, w_support, phase_on=True, threads=0, return_g
         out["grid"] = grid
         out["gridss"] = gridss
     return out
+
+
+def image_chunked(obs, nx, ny, nw, kernel, w_support, phase_on=True, threads=0,
+                  fft_workers=None, progress=None):
+    """The one-rank pipeline of ``image`` one w-plane at a time, with 64-bit
+    indices throughout, for cubes too large to hold (8192^2 x 64 FP64 is 68.7 GB)
+    and past the reference's 32-bit cube indices (w-stacking.cu:168,
+    phase_correction.cu:198).  Per plane iw: the packed rows whose plane is iw by
+    the reference's expression (``plane_of``), in their packing order, are
+    gridded with Nw' = 1 and w' = 0 (w enters wstack only through grid_w,
+    w-stacking.cu:466-469, so the plane's cells receive the same additions in
+    the same order), the plane is transformed, and phase_correction over that
+    plane alone (global iw, the whole cube's dw and dwnorm) accumulates into the
+    image.  Single-threaded, the image has the bits of ``image``."""
+    rows = sector0_rows(obs.vv, obs.meta["Nmeasures"], nx, ny, w_support)
+    uu, vv, ww, w, vr, vi = pack(obs, rows)
+    nchan, npol = obs.meta["freq_per_chan"], obs.meta["polarisations"]
+    nv = nchan * npol
+    dx, dw = 1.0 / nx, 1.0 / nw
+    gw = plane_of(ww, nw)
+    order = np.argsort(gw, kind="stable")
+    bounds = np.searchsorted(gw[order], np.arange(nw + 1))
+    dropped = int(len(gw) - (bounds[nw] - bounds[0]))      # grid_w outside [0, Nw)
+    w2, vr2, vi2 = w.reshape(-1, npol), vr.reshape(-1, nv), vi.reshape(-1, nv)
+    res = resolution_of(obs.meta)
+    img_re, img_im = np.zeros(nx * ny), np.zeros(nx * ny)
+    for iw in range(nw):
+        sel = order[bounds[iw]:bounds[iw + 1]]
+        plane = np.zeros(2 * nx * ny)
+        if len(sel):
+            _, d = wstack(kernel, 1, nchan, npol, uu[sel], vv[sel], np.zeros(len(sel)),
+                          vr2[sel].ravel(), vi2[sel].ravel(), w2[sel].ravel(), dx, dw, w_support,
+                          nx, ny, grid=plane, threads=threads)
+            dropped += d
+        gss = fft_planes(plane, 1, nx, ny, workers=fft_workers)
+        del plane
+        phase_correction_planes(gss, nx, ny, nw, iw, 1, res, obs.meta["wmin"], obs.meta["wmax"],
+                                img_re, img_im, phase_on, threads)
+        if progress:
+            progress(iw)
+    return dict(image_re=img_re, image_im=img_im, rows=len(rows), dropped=dropped)
 
 
 def rel_l2(a, b) -> float:

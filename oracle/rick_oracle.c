@@ -175,16 +175,22 @@ int oracle_wstack(int kernel, int num_w_planes, uint64_t num_points, uint32_t fr
   return 0;
 }
 
-/* phase_correction.cu:97-102, 185-250 (CPU branch, PHASE_ON): the image
- * accumulates, over w-planes, the FFT'd plane times the w-term phase screen
- * times dwnorm*sqrt(1-r^2).  phase_on == 0 or num_w_planes == 1 is a plain
- * sum.  Pixels are processed in any order; for each pixel the planes are
- * summed in increasing iw, which is the reference's order for one thread. */
-int oracle_phase_correction(const double *gridss, double *image_real, double *image_imag,
-                            int xaxis, int yaxis, int num_w_planes, int xaxistot, int yaxistot,
-                            double resolution, double wmin, double wmax, int phase_on,
-                            int num_threads)
+/* phase_correction.cu:97-102, 185-250 (CPU branch, PHASE_ON) for the planes
+ * w_first .. w_first+w_count-1 of a cube of num_w_planes planes: the image
+ * accumulates, over those planes, the FFT'd plane times the w-term phase
+ * screen times dwnorm*sqrt(1-r^2).  gridss holds only those planes (plane
+ * iw at offset (iw - w_first)); dw, dwnorm and wterm are those of the whole
+ * cube.  phase_on == 0 or num_w_planes == 1 is a plain sum.  Pixels are
+ * processed in any order; for each pixel the planes are summed in increasing
+ * iw, which is the reference's order for one thread, and the running sum is
+ * read from and written back to the image, so calls over consecutive plane
+ * ranges give the bits of one call over all planes. */
+int oracle_phase_correction_planes(const double *gridss, double *image_real, double *image_imag,
+                                   int xaxis, int yaxis, int num_w_planes, int w_first,
+                                   int w_count, int xaxistot, int yaxistot, double resolution,
+                                   double wmin, double wmax, int phase_on, int num_threads)
 {
+  if (w_first < 0 || w_count < 0 || w_first + w_count > num_w_planes) return -1;
   const double dw = (wmax - wmin) / (double)num_w_planes;
   const double dwnorm = dw / (wmax - wmin);
   const int64_t plane = (int64_t)xaxis * (int64_t)yaxis;
@@ -205,19 +211,19 @@ int oracle_phase_correction(const double *gridss, double *image_real, double *im
       if (ycoord < 0.0) ycoord = (double)(iv + yaxistot / 2);
       ycoord = sin(ycoord * resolution);
       const double radius2 = (xcoord * xcoord + ycoord * ycoord);
-      for (int iw = 0; iw < num_w_planes; iw++) {
+      for (int iw = w_first; iw < w_first + w_count; iw++) {
         const double wterm = wmin + iw * dw;
         const double preal = cos(2.0 * ORACLE_PI * wterm * (sqrt(1 - radius2) - 1.0));
         const double pimag = sin(2.0 * ORACLE_PI * wterm * (sqrt(1 - radius2) - 1.0));
-        const int64_t index = 2 * (pix + plane * iw);
+        const int64_t index = 2 * (pix + plane * (iw - w_first));
         const double p = gridss[index], q = gridss[index + 1];
         const double r = preal, s = pimag;
         acc_re += (p * r - q * s) * dwnorm * sqrt(1 - radius2);
         acc_im += (p * s + q * r) * dwnorm * sqrt(1 - radius2);
       }
     } else {
-      for (int iw = 0; iw < num_w_planes; iw++) {
-        const int64_t index = 2 * (pix + plane * iw);
+      for (int iw = w_first; iw < w_first + w_count; iw++) {
+        const int64_t index = 2 * (pix + plane * (iw - w_first));
         acc_re += gridss[index];
         acc_im += gridss[index + 1];
       }
@@ -226,6 +232,17 @@ int oracle_phase_correction(const double *gridss, double *image_real, double *im
     image_imag[pix] = acc_im;
   }
   return 0;
+}
+
+/* The whole cube: phase_correction.cu:97-250 as one call. */
+int oracle_phase_correction(const double *gridss, double *image_real, double *image_imag,
+                            int xaxis, int yaxis, int num_w_planes, int xaxistot, int yaxistot,
+                            double resolution, double wmin, double wmax, int phase_on,
+                            int num_threads)
+{
+  return oracle_phase_correction_planes(gridss, image_real, image_imag, xaxis, yaxis,
+                                        num_w_planes, 0, num_w_planes, xaxistot, yaxistot,
+                                        resolution, wmin, wmax, phase_on, num_threads);
 }
 
 /* Rows that one rank grids, in the order it packs them.

@@ -33,12 +33,18 @@ def test_reference_arm_line():
     assert cpu["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "vis/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+    # the same workload keys as our arm's line; timed steps cover measured chunks
+    assert {"workload", "rows", "visibilities", "grid", "w_planes", "kernel", "w_support",
+            "l2", "parallelism", "time_fraction"} <= d["config"].keys()
+    assert abs(d["ms_per_step"] * d["steps"] * 1e-3 * d["value"] -
+               float(cpu["sample"].split("(")[1].split(" jobs")[0]) * d["config"]["visibilities"]
+               ) / (d["config"]["visibilities"]) < 0.05
 
 
 @pytest.mark.gpu
 def test_our_arm_line():
-    d = _line(["--workload", "c1", "--steps", "3", "--warmup", "3", "--no-served", "--no-batched",
-               "--no-cpu-baseline"], 900)
+    d = _line(["--workload", "c1", "--steps", "3", "--warmup", "3", "--no-served", "--no-batched"],
+              900)
     assert (COMMON | {"roofline", "gpu_launches", "clocks"}) <= d.keys()
     assert d["unit"] == "vis/s" and d["value"] > 0 and d["warmup"] >= 3 and d["steps"] == 3
     assert d["dtype"] == "f64" and d["data"] == "synthetic" and d["scaling"] in ("weak", "strong")
@@ -53,3 +59,7 @@ def test_our_arm_line():
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= d["clocks"].keys()
     forms = d["forms"]
     assert forms["mixed"]["rel_l2_vs_fp64"] < 1e-5
+    # both forms against the CPU path's own image of the same job
+    assert forms["vs_oracle"]["fp64"]["rel_l2"] < 1e-12
+    assert forms["vs_oracle"]["mixed"]["rel_l2"] < 1e-5
+    assert d["cpu_baseline"]["value"] > 0 and d["cpu_baseline"]["kind"] in ("reference", "port")
