@@ -117,6 +117,9 @@ def parse():
                     help="N>1: independent jobs per GPU (weak scaling) or one job with its "
                          "w-planes split over the GPUs and the image all-reduced (strong)")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--no-dropin", action="store_true",
+                    help="skip the drop-in leg (wstack + rick_fft_planes + phase_correction on "
+                         "host buffers)")
     ap.add_argument("--served-requests", type=int, default=300)
     ap.add_argument("--served-rates", type=float, nargs="+", default=[250.0, 500.0, 1000.0, 0.0],
                     help="arrival rates (jobs/s) of the served-stream leg; 0 = all at once")
@@ -411,7 +414,7 @@ def run_ours(args):
     in_bytes = sum(int(r.numel() * r.element_size()) for r in rows)
     dense_bytes = 8 * nvis + n * (24 + 4 * npol) + 4 * g8 + 16 * nx * ny
     sparse_bytes = sum(alg[k] for k in stage64 if k in alg)
-    cpu, oracle_err = None, None
+    cpu, oracle_err, dropin, ref_img = None, None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hrows = _host_rows(host if host is not None else rows)
         cpu, ref_img = cpu_baseline(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax)
@@ -426,6 +429,10 @@ def run_ours(args):
                 "rel_l2": float(torch.linalg.vector_norm(im - ref_t) / torch.linalg.vector_norm(ref_t)),
                 "max_abs_rel_to_peak": float((im - ref_t).abs().max() / ref_t.abs().max())}
         del ref_t
+        if not args.no_dropin and args.workload == "c2":
+            hrows = _host_rows(host if host is not None else rows)
+            dropin = run_dropin(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, ref_img)
+            del hrows
     del host
     line = {
         "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": args.steps,
@@ -460,6 +467,7 @@ def run_ours(args):
                 "records": stats64["records"], "work_items": stats64["work_items"],
                 "generate_s": gen_s},
         "cpu_baseline": cpu,
+        "dropin": dropin,
     }
     if not args.no_batched and world == 1:
         ctx, line["batched"] = run_batched(args, dev, stream)
@@ -650,6 +658,62 @@ def _threads():
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+def run_dropin(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, ref_img, steps=2):
+    """The drop-in entry points in the reference's own call sequence, on
+    pageable host buffers as the reference's main allocates them: wstack of
+    every row into a zeroed host cube (gridding_cpu.c:187-204), rick_fft_planes
+    (fftw_data's arithmetic, fourier_transform.c:13-93), phase_correction into
+    zeroed host images (fourier_transform.c:209-216).  One untimed round, then
+    `steps` timed rounds (wall clock: each call synchronises); the counters
+    show whether the timed rounds created a plan or allocated row buffers."""
+    import rick_b200 as R
+    R.set_kernel(cfg.kernel)
+    R.set_phase_on(True)
+    uu, vv, ww, wt, vr, vi = (np.array(a, copy=True) for a in hrows)   # pageable copies
+    n = len(uu)
+    grid = np.empty(2 * nw * nx * ny)
+    gridss = np.empty_like(grid)
+    re, im = np.empty(nx * ny), np.empty(nx * ny)
+
+    def one_round(times):
+        t0 = time.perf_counter()
+        grid.fill(0.0)
+        re.fill(0.0)
+        im.fill(0.0)
+        t1 = time.perf_counter()
+        R.wstack(nw, n, nchan, npol, uu, vv, ww, vr, vi, wt, 1.0 / nx, 1.0 / nw, cfg.w_support,
+                 nx, ny, grid)
+        t2 = time.perf_counter()
+        R.fft_planes(grid, nw, nx, ny, out=gridss)
+        t3 = time.perf_counter()
+        R.phase_correction(gridss, re, im, nx, ny, nw, nx, ny, res, wmin, wmax)
+        t4 = time.perf_counter()
+        times.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
+
+    warm = []
+    one_round(warm)
+    c0 = R.dropin_counters()
+    times = []
+    for _ in range(steps):
+        one_round(times)
+    c1 = R.dropin_counters()
+    tt = np.array(times)
+    job_s = float(tt[:, 1:].sum(axis=1).mean())
+    out = {"workload": "the headline job's rows (all gridded, as wstack grids every row "
+                       "given), 4 host buffers pageable", "steps": steps,
+           "vis_per_s": n * nchan * npol / job_s, "ms_per_job": job_s * 1e3,
+           "ms_wstack": float(tt[:, 1].mean() * 1e3), "ms_fft": float(tt[:, 2].mean() * 1e3),
+           "ms_phase": float(tt[:, 3].mean() * 1e3),
+           "host_bytes_moved_per_job": int(sum(a.nbytes for a in (uu, vv, ww, wt, vr, vi))
+                                           + 5 * grid.nbytes + 4 * re.nbytes),
+           "plans_created_in_timed_rounds": c1["plans_created"] - c0["plans_created"],
+           "row_allocations_in_timed_rounds": c1["row_allocations"] - c0["row_allocations"]}
+    if ref_img is not None:
+        img = np.concatenate([re, im])
+        out["rel_l2_vs_oracle"] = float(np.linalg.norm(img - ref_img) / np.linalg.norm(ref_img))
+    return out
 
 
 class CpuJob:

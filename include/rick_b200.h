@@ -94,6 +94,13 @@ int rick_set_kernel(int kernel);       /* RICK_KERNEL_*; default KAISER_BESSEL *
 int rick_set_phase_on(int on);         /* PHASE_ON; default on */
 int rick_set_device(int device);       /* overrides rank % device_count */
 int rick_last_status(void);            /* status of this thread's last drop-in call */
+/* Drop-in resource accounting (no counterpart in the reference): plans the
+ * drop-ins have created and device allocations of their row buffers, so far
+ * in this process.  The cached plan of a device serves every drop-in call on
+ * the same cube geometry, so a repeated wstack -> rick_fft_planes ->
+ * phase_correction sequence creates and allocates nothing after its first
+ * round. */
+int rick_dropin_counters(uint64_t *plans_created, uint64_t *row_allocations);
 const char *rick_status_string(int status);
 const char *rick_last_error_message(void); /* detail of this thread's last failure */
 
@@ -340,7 +347,18 @@ int rick_server_submit(rick_server *server, const rick_job_desc *job, uint64_t *
 int rick_server_wait(rick_server *server, uint64_t ticket, double timeout_ms,
                      rick_job_result *result);
 int rick_server_get_stats(rick_server *server, rick_server_stats *stats);
-/* Finishes every submitted job, then releases the server. */
+/* Cancels a job still waiting for admission: its wait returns
+ * RICK_ERR_CANCELLED.  A job already launched is never interrupted (no kernel
+ * is stopped part-way); for it, and for unknown tickets, this returns
+ * RICK_ERR_INVALID_ARG and the job completes as usual.  The reference's
+ * counterpart is a failed rank ending the run (main.c:6-28, errcodes.h). */
+int rick_server_cancel(rick_server *server, uint64_t ticket);
+/* Stops admitting jobs: submit returns RICK_ERR_CANCELLED from now on.  With
+ * drain != 0 every waiting job still runs; with drain == 0 the waiting jobs
+ * are cancelled (their waits return RICK_ERR_CANCELLED) while the launched
+ * batches finish.  Does not block. */
+int rick_server_shutdown(rick_server *server, int drain);
+/* Finishes every submitted (and not cancelled) job, then releases the server. */
 int rick_server_destroy(rick_server *server);
 
 /* Page-locked host memory (for the buffers of rick_plan_ingest_samples and

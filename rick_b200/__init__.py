@@ -159,6 +159,9 @@ def lib():
     L.rick_server_wait.argtypes = [_vp, C.c_uint64, C.c_double, C.POINTER(JobResult)]
     L.rick_server_get_stats.argtypes = [_vp, C.POINTER(ServerStats)]
     L.rick_server_destroy.argtypes = [_vp]
+    L.rick_server_cancel.argtypes = [_vp, C.c_uint64]
+    L.rick_dropin_counters.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.rick_server_shutdown.argtypes = [_vp, C.c_int]
     L.rick_normalize_uvw.argtypes = [C.c_uint64, _vp, _vp, _vp, _vp, _vp]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
     L.rick_launch_count.argtypes = []
@@ -171,7 +174,9 @@ def lib():
                "rick_batch_run", "rick_batch_get_tuning", "rick_batch_get_stats",
                "rick_batch_destroy", "rick_batch_kernels_per_run", "rick_server_create",
                "rick_server_submit", "rick_server_wait", "rick_server_get_stats",
-               "rick_server_destroy", "rick_normalize_uvw", "rick_plan_ingest_begin",
+               "rick_server_destroy", "rick_server_cancel", "rick_server_shutdown",
+               "rick_dropin_counters",
+               "rick_normalize_uvw", "rick_plan_ingest_begin",
                "rick_plan_ingest_samples", "rick_plan_ingest_end", "rick_host_alloc",
                "rick_host_free"]:
         getattr(L, fn).restype = C.c_int
@@ -241,6 +246,13 @@ def phase_correction(gridss, image_real, image_imag, xaxis, yaxis, num_w_planes,
                            rank)
     check(lib().rick_last_status(), "phase_correction")
     return image_real, image_imag
+
+
+def dropin_counters() -> dict:
+    """Plans the drop-ins created and their row-buffer allocations so far."""
+    a, b = C.c_uint64(), C.c_uint64()
+    check(lib().rick_dropin_counters(C.byref(a), C.byref(b)), "rick_dropin_counters")
+    return {"plans_created": int(a.value), "row_allocations": int(b.value)}
 
 
 def fft_planes(grid, num_w_planes, grid_size_x, grid_size_y, out=None):
@@ -523,6 +535,20 @@ class Server:
         check(st, "rick_server_wait")
         return {k: (float(getattr(r, k)) if k.endswith("_ms") else int(getattr(r, k)))
                 for k, _ in JobResult._fields_}
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a job still waiting for admission (its wait then raises
+        RickError with ERR_CANCELLED); False when it was already launched."""
+        st = lib().rick_server_cancel(self._h, ticket)
+        if st == ERR_INVALID_ARG:
+            return False
+        check(st, "rick_server_cancel")
+        return True
+
+    def shutdown(self, drain: bool = True):
+        """Stops admitting jobs; with drain=False the waiting ones are cancelled
+        while launched batches finish (include/rick_b200.h)."""
+        check(lib().rick_server_shutdown(self._h, int(bool(drain))), "rick_server_shutdown")
 
     def stats(self) -> dict:
         s = ServerStats()

@@ -220,12 +220,24 @@ __device__ __forceinline__ void scatter_rows(
   const unsigned lane = lane_id();
   const unsigned sub = lane % G, grp = lane / G;
   const uint64_t nv = (uint64_t)nchan * npol;
+  // where the lane's own row goes, before any sample is read: rows that reach
+  // no tile (dropped, outside the sector, of another shard's planes, or with
+  // the footprint off the grid) never stream their samples
+  const uint64_t i_own = base + lane;
+  RowPos p;
+  p.keep = false;
+  p.other = false;
+  if (i_own < nrows) p = row_position(uu[i_own], vv[i_own], ww[i_own], g);
+  uint32_t bins[4];
+  footprint_bins(p, g, bins);
+  const bool need = bins[0] != kNoBin;
   double my_re = 0.0, my_im = 0.0;
 #pragma unroll 1
   for (int round = 0; round < G; round++) {
     const uint64_t i = base + (uint64_t)round * R + grp;
     double sre = 0.0, sim = 0.0;
-    if (i < nrows) {
+    const bool need_i = __shfl_sync(kFull, need, round * R + grp);
+    if (i < nrows && need_i) {
       const float *wrow = weight + i * npol;
       if (V4) {
         // npol divides 4, so component c of every float4 is polarisation c % npol
@@ -274,12 +286,6 @@ __device__ __forceinline__ void scatter_rows(
     }
   }
 
-  const uint64_t i = base + lane;
-  RowPos p;
-  p.keep = false;
-  if (i < nrows) p = row_position(uu[i], vv[i], ww[i], g);
-  uint32_t bins[4];
-  footprint_bins(p, g, bins);
   offset_bins(bins, bin_base);
   gridded += p.keep ? 1u : 0u;
   RecF64 r;

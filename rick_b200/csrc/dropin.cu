@@ -37,6 +37,8 @@ int g_device = -1;     // -1: rank % device_count
 thread_local int g_last_status = RICK_OK;
 constexpr int kMaxDevices = 64;
 rick_plan *g_plans[kMaxDevices] = {};
+uint64_t g_plans_created = 0;   // plans the drop-ins have created in this process
+uint64_t g_row_allocs = 0;      // device allocations of their row buffers
 double *g_dimg[kMaxDevices] = {};
 uint64_t g_dimg_vals[kMaxDevices] = {};
 
@@ -75,16 +77,26 @@ int pick_device(int rank, int *dev) {
   return RICK_OK;
 }
 
-// Cached plan for (device, geometry); re-created when the geometry changes or
-// the row capacity is too small.
-int get_plan(int dev, int nx, int ny, int nw, int support, int kernel, uint64_t rows,
+// The cached plan of a device serves every drop-in call on the same cube:
+// wstack needs its gridding settings (support, kernel, channels,
+// polarisations, row capacity) as well; rick_fft_planes and phase_correction
+// need only the cube's geometry and the PHASE_ON setting, so the reference's
+// call sequence wstack -> fft -> phase_correction, repeated, reuses one plan
+// (and its HBM) throughout.  A plan is re-created only when a call needs
+// something the cached one lacks.
+enum class Need { kGrid, kCube };
+
+int get_plan(int dev, Need need, int nx, int ny, int nw, int support, int kernel, uint64_t rows,
              uint32_t nchan, uint32_t npol, rick_plan **out) {
   rick_plan *p = g_plans[dev];
   if (p) {
     const rick_plan_desc *d = rick_internal_plan_desc(p);
-    if (d->grid_size_x != nx || d->grid_size_y != ny || d->num_w_planes != nw ||
-        d->w_support != support || d->kernel != kernel || d->max_rows < rows ||
-        d->freq_per_chan != nchan || d->polarizations != npol || d->phase_on != phase_setting()) {
+    bool ok = d->grid_size_x == nx && d->grid_size_y == ny && d->num_w_planes == nw &&
+              d->phase_on == phase_setting();
+    if (need == Need::kGrid)
+      ok = ok && d->w_support == support && d->kernel == kernel && d->max_rows >= rows &&
+           d->freq_per_chan == nchan && d->polarizations == npol;
+    if (!ok) {
       rick_plan_destroy(p);
       g_plans[dev] = p = nullptr;
     }
@@ -104,26 +116,37 @@ int get_plan(int dev, int nx, int ny, int nw, int support, int kernel, uint64_t 
     d.polarizations = npol;
     RICK_TRY(rick_plan_create(&p, &d));
     g_plans[dev] = p;
+    g_plans_created++;
   }
   *out = p;
   return RICK_OK;
 }
 
-template <typename T>
-struct DevBuf {
-  T *ptr = nullptr;
-  ~DevBuf() {
-    if (ptr) cudaFree(ptr);
-  }
-  int alloc(uint64_t n) {
-    cudaError_t e = cudaMalloc(&ptr, n * sizeof(T) + 16);
-    if (e != cudaSuccess) {
-      ptr = nullptr;
-      return cuda_status(e, "cudaMalloc", __FILE__, __LINE__);
-    }
-    return RICK_OK;
-  }
+// Device copies of wstack's row arrays, kept per device across calls and grown
+// (with headroom) when a call brings more rows or samples.
+struct RowBufs {
+  double *uvw = nullptr;
+  float *wt = nullptr, *vr = nullptr, *vi = nullptr;
+  uint64_t cap_uvw = 0, cap_wt = 0, cap_vr = 0, cap_vi = 0;
 };
+RowBufs g_rows[kMaxDevices];
+
+template <typename T>
+int grow(T **ptr, uint64_t *cap, uint64_t n) {
+  if (*cap >= n && *ptr) return RICK_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *cap = 0;
+  const uint64_t want = n + n / 4 + 16;
+  const cudaError_t e = cudaMalloc((void **)ptr, want * sizeof(T));
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    return cuda_status(e, "cudaMalloc", __FILE__, __LINE__);
+  }
+  g_row_allocs++;
+  *cap = want;
+  return RICK_OK;
+}
 
 int do_wstack(int nw, unsigned int npts, unsigned int nchan, unsigned int npol, const double *uu,
               const double *vv, const double *ww, const float *vr, const float *vi,
@@ -137,14 +160,16 @@ int do_wstack(int nw, unsigned int npts, unsigned int nchan, unsigned int npol, 
   int dev = 0;
   RICK_TRY(pick_device(rank, &dev));
   rick_plan *p = nullptr;
-  RICK_TRY(get_plan(dev, nx, ny, nw, support, kernel_setting(), npts, nchan, npol, &p));
+  RICK_TRY(get_plan(dev, Need::kGrid, nx, ny, nw, support, kernel_setting(), npts, nchan, npol,
+                    &p));
   const uint64_t nv = (uint64_t)npts * nchan * npol;
-  DevBuf<double> duvw;
-  DevBuf<float> dwt, dvr, dvi;
-  RICK_TRY(duvw.alloc(3ull * npts));
-  RICK_TRY(dwt.alloc((uint64_t)npts * npol));
-  RICK_TRY(dvr.alloc(nv));
-  RICK_TRY(dvi.alloc(nv));
+  RowBufs &b = g_rows[dev];
+  RICK_TRY(grow(&b.uvw, &b.cap_uvw, 3ull * npts));
+  RICK_TRY(grow(&b.wt, &b.cap_wt, (uint64_t)npts * npol));
+  RICK_TRY(grow(&b.vr, &b.cap_vr, nv));
+  RICK_TRY(grow(&b.vi, &b.cap_vi, nv));
+  struct { double *ptr; } duvw{b.uvw};
+  struct { float *ptr; } dwt{b.wt}, dvr{b.vr}, dvi{b.vi};
   cudaStream_t st = 0;
   RICK_CUDA(cudaMemcpyAsync(duvw.ptr, uu, npts * 8ull, cudaMemcpyHostToDevice, st));
   RICK_CUDA(cudaMemcpyAsync(duvw.ptr + npts, vv, npts * 8ull, cudaMemcpyHostToDevice, st));
@@ -172,7 +197,7 @@ int do_phase(double *gridss, double *img_re, double *img_im, int xaxis, int yaxi
   int dev = 0;
   RICK_TRY(pick_device(rank, &dev));
   rick_plan *p = nullptr;
-  RICK_TRY(get_plan(dev, xaxis, yaxis, nw, 7, kernel_setting(), 1, 1, 1, &p));
+  RICK_TRY(get_plan(dev, Need::kCube, xaxis, yaxis, nw, 7, kernel_setting(), 1, 1, 1, &p));
   const uint64_t plane = (uint64_t)xaxis * yaxis;
   if (g_dimg_vals[dev] < 2 * plane) {
     if (g_dimg[dev]) cudaFree(g_dimg[dev]);
@@ -202,7 +227,7 @@ int do_fft(const double *grid, double *gridss, int nw, int nx, int ny) {
   int dev = 0;
   RICK_TRY(pick_device(0, &dev));
   rick_plan *p = nullptr;
-  RICK_TRY(get_plan(dev, nx, ny, nw, 7, kernel_setting(), 1, 1, 1, &p));
+  RICK_TRY(get_plan(dev, Need::kCube, nx, ny, nw, 7, kernel_setting(), 1, 1, 1, &p));
   cudaStream_t st = 0;
   RICK_TRY(rick_plan_import_cube(p, grid, 1, st));
   RICK_TRY(rick_internal_plan_mark_raw(p));
@@ -270,6 +295,13 @@ int rick_set_device(int device) {
 
 int rick_last_status(void) { return g_last_status; }
 
+int rick_dropin_counters(uint64_t *plans_created, uint64_t *row_allocations) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (plans_created) *plans_created = g_plans_created;
+  if (row_allocations) *row_allocations = g_row_allocs;
+  return RICK_OK;
+}
+
 const char *rick_status_string(int status) {
   switch (status) {
     case RICK_OK: return "ok";
@@ -313,7 +345,7 @@ int rick_kernel_names(const char **names, int max_names) {
   static const char *k[] = {"k_bin_count",        "k_item_count",       "k_bin_scatter",
                             "k_scan_block",       "k_scan_add",         "k_grid_tiles",
                             "k_zero_split_tiles", "k_row_list",         "k_fft_units",
-                            "k_fft_rows",         "k_fft_cols_image",   "k_phase_sum",
+                            "k_fft_rows",         "k_fft_cols_image",   "k_fft_cols_tm",      "k_phase_sum",
                             "k_export_cube",      "k_import_cube",      "k_bin_count_batch",
                             "k_bin_scatter_batch", "k_grid_tiles_batch", "k_zero_split_tiles_batch",
                             "k_fft_rows_multi",   "k_fft_cols_multi",   "k_uvw_init",

@@ -18,6 +18,7 @@
 // with FP64 twiddles computed on the host in long double.  Power-of-two sizes
 // from 64 to 8192; other sizes use the cuFFT plan.
 #include <math.h>
+#include <stdlib.h>
 
 #include <algorithm>
 
@@ -356,8 +357,8 @@ __device__ __forceinline__ void fft_inplace(typename V2<T>::t *s, int t,
   if (REM == 2) stockham_pass<T, N, 4>(s, t, Ns, tw);
 }
 
-template <int LOGN> constexpr int group_threads() { return (1 << LOGN) / kVpt; }
-template <int LOGN> constexpr int block_threads() {
+template <int LOGN> __host__ __device__ constexpr int group_threads() { return (1 << LOGN) / kVpt; }
+template <int LOGN> __host__ __device__ constexpr int block_threads() {
   return group_threads<LOGN>() > 256 ? group_threads<LOGN>() : 256;
 }
 // Blocks of 256 threads (lengths up to 2048) are bounded to 128 registers so
@@ -719,6 +720,292 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
   __syncthreads();  // sstep / smask are rewritten for the next column
 }
 
+// ---- Column pass with the per-pixel state in tensor memory ---------------
+//
+// The w-correction as a Horner recurrence over the planes, walked in
+// decreasing w: with s = exp(i 2 pi dw (root - 1)) the per-pixel factor
+// between consecutive planes and P = dwnorm root exp(i 2 pi wterm_lo (root-1))
+// the factor of the lowest plane with data,
+//     image = P * (((x_hi s^g + ...) s^g' + x_lo)
+// so each pixel carries two complex values across planes -- its running sum
+// and its step s -- and the phase needs one sincos per pixel for s and one
+// for P per column, none per plane.  The reference evaluates every plane's
+// factor with its own sincos (phase_correction.cu:205-226); the recurrence's
+// products move each factor by a few ulp per plane (< 1e-13 relative over 64
+// planes of a 8192^2 wide-field image), below the rounding of the reference's
+// own phase argument.
+//
+// The two complex values of the thread's 8 pixels (64 32-bit words) live in
+// tensor memory (TMEM, 512 columns x 128 lanes of 32 bits per SM), not in
+// registers: the thread's FFT then runs in 64 registers, so 1024 threads
+// share an SM (two 4096-point columns, four blocks of shorter ones) where the
+// register-resident form held one.  Warp w of a block reaches lanes
+// 32 (w % 4) .. +31 (its lane quarter); the warps of one quarter split its
+// columns, 64 each, so a block allocates (warps / 4) * 64 columns and two,
+// one or four blocks fill an SM's 512.  Column loads are single-buffered: the
+// next plane's copies are issued as soon as the FFT's last pass has read the
+// buffer and land during the recurrence, and the other blocks of the SM
+// overlap the rest.
+namespace tm {
+
+__device__ __forceinline__ void alloc(uint32_t *smem_dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// 8 consecutive columns of the thread's lane; the registers are ready after
+// wait_ld8, which names them so that no use moves above the wait.
+__device__ __forceinline__ void ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void wait_ld8(uint32_t (&a)[8], uint32_t (&b)[8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]),
+                 "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void wait_ld8(uint32_t (&a)[8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(
+                   taddr),
+               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+               "r"(r[7])
+               : "memory");
+}
+// The stored registers stay untouched until the store has completed.
+__device__ __forceinline__ void wait_st8(uint32_t (&r)[8]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7])
+               :
+               : "memory");
+}
+
+__device__ __forceinline__ double join(uint32_t lo, uint32_t hi) {
+  return __hiloint2double((int)hi, (int)lo);
+}
+__device__ __forceinline__ void split(double v, uint32_t &lo, uint32_t &hi) {
+  lo = (uint32_t)__double2loint(v);
+  hi = (uint32_t)__double2hiint(v);
+}
+
+}  // namespace tm
+
+// TMEM columns a block of `threads` allocates: 64 per warp of a lane quarter.
+__host__ __device__ constexpr uint32_t tm_cols(int threads) {
+  return (uint32_t)(threads / 32 / 4) * 64u;
+}
+
+template <int LOGN>
+__host__ __device__ constexpr size_t cols_tm_smem_bytes(int rpc) {
+  return (size_t)rpc * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(double2) + 16;
+}
+
+// Columns base..base+rpc-1 of one job (one per row group), FP64.
+// `taddr` is the thread's TMEM address: its lane quarter and its warp's 64
+// columns -- [0, 32) the 8 running sums, [32, 64) the 8 steps, 4 words each
+// (re lo/hi, im lo/hi), pixel q at 4q.
+template <int LOGN>
+__device__ __forceinline__ void fft_col_unit_tm(double2 *s, uint32_t base, const ColJob<double> &J,
+                                                uint32_t taddr) {
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  constexpr int CB = col_block<double>();
+  using V = double2;
+  const int grp = threadIdx.x / G, t = threadIdx.x % G;
+  const int nx = J.nx, ny = J.ny, nw = J.nw, nty = J.nty;
+  const uint32_t *__restrict__ counts = J.counts;
+  V *buf = s + grp * LEN;
+  const uint32_t n = base + grp;
+  const bool active = n < (uint32_t)nx;
+  const bool phase = J.phase_on && J.nw_total > 1;
+  const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
+  auto prev_plane = [&](int iw) {   // planes without data add exact zeros
+    do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
+    return iw;
+  };
+  // the touched rows of plane iw into the buffer (untouched rows zero-filled)
+  auto load_plane = [&](int iw) {
+    const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
+    const V *col = J.cube + blocked_index<double>(iw, 0, active ? n : 0, nx, ny);
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      const int k = t + q * G;
+      const bool touched = active && ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u);
+      cp_async_zfill<double>(buf + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
+    }
+    cp_async_commit();
+  };
+  // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits
+  const double l = active ? J.ltab[n] : 0.0;
+  auto root_of = [&](int m) {
+    const double mm = J.mtab[m];
+    return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
+  };
+  int iw = prev_plane(nw);
+  if (iw >= 0) load_plane(iw);
+  // the per-pixel steps into TMEM
+  const double dwstep = __dmul_rn(twopi, J.dw);
+#pragma unroll
+  for (int h = 0; h < kVpt / 2; h++) {
+    uint32_t w8[8];
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int m = t + (2 * h + e) * G;
+      double sn = 0.0, cs = 1.0;
+      if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(m), 1.0)), &sn, &cs);
+      tm::split(cs, w8[4 * e + 0], w8[4 * e + 1]);
+      tm::split(sn, w8[4 * e + 2], w8[4 * e + 3]);
+    }
+    tm::st8(taddr + 32 + 8 * h, w8);
+    tm::wait_st8(w8);
+  }
+  bool first = true;
+  int prev = iw;
+  while (iw >= 0) {
+    cp_async_wait<0>();
+    __syncthreads();  // the plane's copies have landed in every thread's rows
+    Cx<double> x[kVpt];
+    fft_to_regs<double, LOGN>(buf, t, J.tw, x);
+    __syncthreads();  // every thread has read the buffer
+    const int nxt = prev_plane(iw);
+    if (nxt >= 0) load_plane(nxt);
+    const int gap = prev - iw;
+#pragma unroll
+    for (int h = 0; h < kVpt / 2; h++) {
+      uint32_t a8[8], s8[8];
+      if (first) {
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          tm::split(x[2 * h + e].re, a8[4 * e + 0], a8[4 * e + 1]);
+          tm::split(x[2 * h + e].im, a8[4 * e + 2], a8[4 * e + 3]);
+        }
+      } else {
+        tm::ld8(taddr + 8 * h, a8);
+        tm::ld8(taddr + 32 + 8 * h, s8);
+        tm::wait_ld8(a8, s8);
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          double ar = tm::join(a8[4 * e + 0], a8[4 * e + 1]);
+          double ai = tm::join(a8[4 * e + 2], a8[4 * e + 3]);
+          const double sr = tm::join(s8[4 * e + 0], s8[4 * e + 1]);
+          const double si = tm::join(s8[4 * e + 2], s8[4 * e + 3]);
+          for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
+            const double tr = fma(ar, sr, -ai * si);
+            ai = fma(ar, si, ai * sr);
+            ar = tr;
+          }
+          const double nr = fma(ar, sr, fma(-ai, si, x[2 * h + e].re));
+          const double ni = fma(ar, si, fma(ai, sr, x[2 * h + e].im));
+          tm::split(nr, a8[4 * e + 0], a8[4 * e + 1]);
+          tm::split(ni, a8[4 * e + 2], a8[4 * e + 3]);
+        }
+      }
+      tm::st8(taddr + 8 * h, a8);
+      tm::wait_st8(a8);
+    }
+    first = false;
+    prev = iw;
+    iw = nxt;
+  }
+  // image = norm * P * sum, P the factor of the lowest plane with data
+  const double cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + prev), J.dw)));
+#pragma unroll
+  for (int h = 0; h < kVpt / 2; h++) {
+    uint32_t a8[8];
+    if (!first) {
+      tm::ld8(taddr + 8 * h, a8);
+      tm::wait_ld8(a8);
+    }
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int m = t + (2 * h + e) * G;
+      double re = 0.0, im = 0.0;
+      if (!first) {
+        const double ar = tm::join(a8[4 * e + 0], a8[4 * e + 1]);
+        const double ai = tm::join(a8[4 * e + 2], a8[4 * e + 3]);
+        double pr = 1.0, pi = 0.0;
+        if (phase) {
+          const double root = root_of(m);
+          double sn, cs;
+          sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+          const double amp = J.dwnorm * root;
+          pr = cs * amp;
+          pi = sn * amp;
+        }
+        re = J.norm * fma(ar, pr, -ai * pi);
+        im = J.norm * fma(ar, pi, ai * pr);
+      }
+      if (active) {
+        J.img_re[(uint64_t)m * nx + n] = re;
+        J.img_im[(uint64_t)m * nx + n] = im;
+      }
+    }
+  }
+}
+
+template <int LOGN> constexpr int tm_min_blocks() { return 1024 / block_threads<LOGN>(); }
+
+template <int LOGN>
+__global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
+    k_fft_cols_tm(ColJob<double> J) {
+  constexpr int G = (1 << LOGN) / kVpt;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto *s = reinterpret_cast<double2 *>(smem_raw);
+  const int rpc = blockDim.x / G;
+  // the TMEM address slot sits after the column buffers
+  uint32_t *slot = reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<LOGN>(rpc) - 16);
+  constexpr uint32_t ncols = tm_cols(block_threads<LOGN>());
+  const int warp = threadIdx.x / 32;
+  if (warp == 0) {
+    tm::alloc(slot, ncols);
+    tm::relinquish();
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 64u;
+  for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)J.nx; base += gridDim.x * rpc) {
+    fft_col_unit_tm<LOGN>(s, base, J, taddr);
+    __syncthreads();  // the column buffers are rewritten for the next columns
+  }
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    tm::dealloc(tbase, ncols);
+  }
+}
+
 // One job's column pass (the plan): the job as a kernel parameter.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __global__ void __launch_bounds__(block_threads<LOGN>(), col_min_blocks<T, LOGN, PP>())
@@ -924,6 +1211,46 @@ int launch_cols_impl(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
+// One job's FP64 column pass with the per-pixel state in TMEM.  The dynamic
+// shared memory is padded so that shared memory, not the TMEM allocation,
+// bounds the blocks per SM at 512 / (columns a block allocates): a further
+// block could not allocate and would wait for one of the others to finish.
+template <int LOGN>
+int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
+  constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
+  const int rpc = BT / G;
+  const int max_blocks = (int)(512u / tm_cols(BT));
+  int dev = 0, smem_sm = 0, reserved = 0;
+  RICK_CUDA(cudaGetDevice(&dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  size_t sm = cols_tm_smem_bytes<LOGN>(rpc);
+  const size_t floor_b = (size_t)smem_sm / (size_t)(max_blocks + 1) + 1;
+  if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
+  sm = (sm + 15) & ~(size_t)15;
+  RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_tm<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sm));
+  int per_sm = 0;
+  RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_cols_tm<LOGN>, BT, sm));
+  per_sm = std::min(std::max(per_sm, 1), max_blocks);
+  const int blocks = (int)std::min<uint64_t>(std::max<uint32_t>(c.units, 1),
+                                             (uint64_t)num_sms() * per_sm);
+  ColJob<double> J = col_job<double>(*f.one, f);
+  // the slot of the TMEM address sits in the last 16 bytes of the unpadded layout
+  RICK_LAUNCHED();
+  k_fft_cols_tm<LOGN><<<blocks, BT, sm, st>>>(J);
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
+bool cols_tm_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("RICK_COLS_TMEM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename T, int LOGN>
 int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
@@ -931,6 +1258,9 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   // in order of preference, the first that fits: two planes per iteration
   // (FP32), double-buffered loads, the per-pixel phase steps
   constexpr size_t kMax = 220 * 1024;
+  if constexpr (sizeof(T) == 8) {
+    if (f.one && cols_tm_enabled()) return launch_cols_tm<LOGN>(f, c, st);
+  }
 #define RICK_TRY_COLS(DB, RC, PP)                            \
   if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)           \
     return launch_cols_impl<T, LOGN, DB, RC, PP>(f, c, st);

@@ -338,8 +338,37 @@ int rick_server_wait(rick_server *s, uint64_t ticket, double timeout_ms, rick_jo
     res->batch_id = j.batch;
     res->batch_jobs = j.batch_jobs;
   }
+  if (j.status == RICK_ERR_CANCELLED)
+    return set_error(j.status, "job %llu was cancelled before it was launched",
+                     (unsigned long long)ticket);
   return j.status == RICK_OK ? RICK_OK
                              : set_error(j.status, "job %llu failed", (unsigned long long)ticket);
+}
+
+int rick_server_cancel(rick_server *s, uint64_t ticket) {
+  if (!s) return set_error(RICK_ERR_INVALID_ARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+    if (*it != ticket) continue;
+    s->pending.erase(it);
+    fail_jobs(s, {ticket}, RICK_ERR_CANCELLED);
+    return RICK_OK;
+  }
+  return set_error(RICK_ERR_INVALID_ARG, "ticket %llu is not waiting (unknown, launched or done)",
+                   (unsigned long long)ticket);
+}
+
+int rick_server_shutdown(rick_server *s, int drain) {
+  if (!s) return set_error(RICK_ERR_INVALID_ARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->stop = true;
+  if (!drain) {
+    std::vector<uint64_t> waiting(s->pending.begin(), s->pending.end());
+    s->pending.clear();
+    fail_jobs(s, waiting, RICK_ERR_CANCELLED);
+  }
+  s->cv.notify_all();
+  return RICK_OK;
 }
 
 int rick_server_get_stats(rick_server *s, rick_server_stats *out) {

@@ -59,10 +59,14 @@ class ShardedImager:
 
     ``image`` runs this rank's planes through a plan (device-resident rows) and
     all-reduces the image over ``group`` (torch.distributed; NCCL for CUDA
-    tensors), so every rank ends with the whole image."""
+    tensors), so every rank ends with the whole image.  ``plan_factory``
+    builds the rank's plan (default ``rick_b200.Plan``; called as
+    ``plan_factory(geom, max_rows, freq_per_chan, polarizations, device=...,
+    planes=(w_first, w_count))``)."""
 
     def __init__(self, geom, max_rows: int, freq_per_chan: int, polarizations: int,
-                 device: int = 0, group=None, ranges: Optional[list] = None):
+                 device: int = 0, group=None, ranges: Optional[list] = None,
+                 plan_factory=None):
         import torch.distributed as dist
         import rick_b200 as R
 
@@ -74,8 +78,9 @@ class ShardedImager:
         self.world = world
         self.plan = None
         if self.planes[1] > 0:
-            self.plan = R.Plan(geom, max_rows, freq_per_chan, polarizations, device=device,
-                               planes=self.planes)
+            factory = plan_factory if plan_factory is not None else R.Plan
+            self.plan = factory(geom, max_rows, freq_per_chan, polarizations, device=device,
+                                planes=self.planes)
         self.geom = geom
 
     def image(self, nrows, rows, resolution, wmin, wmax, image, selection=None, stream=None):

@@ -313,3 +313,31 @@ def test_grid_and_plane_edges_match_oracle():
                             selection=R.ROWS_ALL)
         assert rel_l2(grid, want) < TOL_FP64, kernel
         assert st["rows_dropped"] == dropped > 0, kernel
+
+
+def test_dropin_sequence_reuses_one_plan(golden):
+    """The reference's call sequence through the drop-ins -- wstack
+    (gridding_cpu.c:187-204), rick_fft_planes, phase_correction
+    (fourier_transform.c:209-216) -- twice on the same cube: the image equals
+    the reference's each time, and the second round creates no plan and
+    allocates no row buffer (one cached plan serves all three calls)."""
+    g = golden(CASES[0])
+    nx, ny, nw = g["nx"], g["ny"], g["nw"]
+    R.set_kernel(g["kernel"])
+    R.set_phase_on(True)
+    uu, vv, ww, wt, vr, vi = _packed_host(g)
+
+    def one_round():
+        grid = np.zeros(2 * nw * nx * ny)
+        R.wstack(nw, len(uu), g["nchan"], g["npol"], uu, vv, ww, vr, vi, wt, 1.0 / nx, 1.0 / nw,
+                 g["support"], nx, ny, grid)
+        gridss = R.fft_planes(grid, nw, nx, ny)
+        re, im = np.zeros(nx * ny), np.zeros(nx * ny)
+        R.phase_correction(gridss, re, im, nx, ny, nw, nx, ny, g["resolution"], g["wmin"],
+                           g["wmax"])
+        assert rel_l2(re, g["image_re"]) < TOL_FP64 and rel_l2(im, g["image_im"]) < TOL_FP64
+
+    one_round()
+    before = R.dropin_counters()
+    one_round()
+    assert R.dropin_counters() == before

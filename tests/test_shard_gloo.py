@@ -5,7 +5,9 @@ own arithmetic restated in C) into a cube whose other planes stay empty, the
 ranks all-reduce their images, and the sum equals the unsharded image.  This
 covers the partition rules and the exchange step of rick_b200.shard; the CUDA
 side of a shard (rick_plan_desc.w_first / w_count) is checked against the same
-identity in test_gpu_shard.py."""
+identity in test_gpu_shard.py.  ``ShardedImager`` itself (its plane choice,
+the zero image of a rank without planes, and its all-reduce) runs over gloo
+with an oracle-backed stand-in for the CUDA plan."""
 import os
 import socket
 
@@ -96,3 +98,62 @@ def test_plane_ranges_partition_the_cube():
     assert b[0] == (0, 1)                      # the heavy first plane alone
     rows = [sum(counts[f:f + c]) for f, c in b]
     assert max(rows) <= 500
+
+
+class _OraclePlan:
+    """CPU stand-in for rick_b200.Plan with a w-plane shard: the oracle images
+    the rows of planes w_first .. w_first+w_count-1 (whole-cube dw, global
+    plane index), as rick_plan_image does for a shard plan."""
+
+    def __init__(self, geom, max_rows, nchan, npol, device=0, planes=(0, 0)):
+        self.first, self.count = planes
+
+    def image(self, nrows, rows, res, wmin, wmax, img_re, img_im, sel, stream=None):
+        import torch
+        img = _partial(tuple(np.asarray(r) for r in rows), self.first, self.count)
+        n = GEOM["nx"] * GEOM["ny"]
+        img_re.copy_(torch.from_numpy(img[:n]))
+        img_im.copy_(torch.from_numpy(img[n:]))
+
+    def close(self):
+        pass
+
+
+def _imager_rank(rank, world, port, nw_ranges, out_dir):
+    import torch
+    import torch.distributed as dist
+    import rick_b200 as R
+    from rick_b200.shard import ShardedImager
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    g = GEOM
+    geom = R.Geometry(g["nx"], g["ny"], g["nw"], g["sup"], g["kernel"], "fp64")
+    rows = _rows()
+    imager = ShardedImager(geom, len(rows[0]), g["nchan"], g["npol"], ranges=nw_ranges,
+                           plan_factory=_OraclePlan)
+    img = torch.full((2 * g["nx"] * g["ny"],), float("nan"), dtype=torch.float64)
+    imager.image(len(rows[0]), rows, g["res"], g["wmin"], g["wmax"], img)
+    np.save(os.path.join(out_dir, f"imager{rank}.npy"), img.numpy())
+    np.save(os.path.join(out_dir, f"planes{rank}.npy"), np.array(imager.planes))
+    imager.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("ranges", [None, [(0, 6), (6, 0)]])
+def test_sharded_imager_reduces_over_gloo(tmp_path, ranges):
+    """Two gloo ranks each build a ShardedImager (even split, or every plane on
+    rank 0 and none on rank 1) and call its image(): both end with the whole
+    image (<= 1e-12 against the unsharded oracle image)."""
+    world = 2
+    mp.start_processes(_imager_rank, args=(world, _free_port(), ranges, str(tmp_path)),
+                       nprocs=world, start_method="spawn", join=True)
+    whole = _partial(_rows(), 0, GEOM["nw"])
+    want = [shard.plane_range(r, world, GEOM["nw"]) for r in range(world)] if ranges is None \
+        else ranges
+    for r in range(world):
+        assert tuple(np.load(tmp_path / f"planes{r}.npy")) == tuple(want[r])
+        got = np.load(tmp_path / f"imager{r}.npy")
+        assert O.rel_l2(got, whole) < 1e-12
