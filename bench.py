@@ -699,6 +699,7 @@ def run_dropin(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, ref_img, st
     for _ in range(steps):
         one_round(times)
     c1 = R.dropin_counters()
+    R.dropin_release()   # its plan and buffers (~28 GB at this size) leave the device
     tt = np.array(times)
     job_s = float(tt[:, 1:].sum(axis=1).mean())
     out = {"workload": "the headline job's rows (all gridded, as wstack grids every row "

@@ -101,6 +101,12 @@ int rick_last_status(void);            /* status of this thread's last drop-in c
  * phase_correction sequence creates and allocates nothing after its first
  * round. */
 int rick_dropin_counters(uint64_t *plans_created, uint64_t *row_allocations);
+/* Frees what the drop-ins keep between calls (the cached plans, row and image
+ * buffers of every device); the next drop-in call starts afresh.  No
+ * counterpart in the reference, whose wstack and phase_correction allocate
+ * and free their device memory on every call (w-stacking.cu:316-331, 420-429;
+ * phase_correction.cu:137-179). */
+int rick_dropin_release(void);
 const char *rick_status_string(int status);
 const char *rick_last_error_message(void); /* detail of this thread's last failure */
 
@@ -277,8 +283,9 @@ typedef struct rick_job_desc {
 } rick_job_desc;
 
 /* Schedule knobs of a batch: gridder records per work item, gridder blocks per
- * SM, and w-planes the column pass keeps in flight per iteration (1 or 2; 2 is
- * used by the mixed form only). */
+ * SM, and the column pass's form: planes_in_flight 0 keeps each pixel's running
+ * sum and w-step in tensor memory (one plane per iteration); 1 or 2 keep them
+ * in registers with that many planes per iteration (2: mixed form only). */
 typedef struct rick_batch_tuning {
   uint32_t max_chunk;
   int grid_blocks_per_sm;

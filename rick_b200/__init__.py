@@ -161,6 +161,7 @@ def lib():
     L.rick_server_destroy.argtypes = [_vp]
     L.rick_server_cancel.argtypes = [_vp, C.c_uint64]
     L.rick_dropin_counters.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.rick_dropin_release.argtypes = []
     L.rick_server_shutdown.argtypes = [_vp, C.c_int]
     L.rick_normalize_uvw.argtypes = [C.c_uint64, _vp, _vp, _vp, _vp, _vp]
     L.rick_kernel_names.argtypes = [C.POINTER(C.c_char_p), C.c_int]
@@ -175,7 +176,7 @@ def lib():
                "rick_batch_destroy", "rick_batch_kernels_per_run", "rick_server_create",
                "rick_server_submit", "rick_server_wait", "rick_server_get_stats",
                "rick_server_destroy", "rick_server_cancel", "rick_server_shutdown",
-               "rick_dropin_counters",
+               "rick_dropin_counters", "rick_dropin_release",
                "rick_normalize_uvw", "rick_plan_ingest_begin",
                "rick_plan_ingest_samples", "rick_plan_ingest_end", "rick_host_alloc",
                "rick_host_free"]:
@@ -253,6 +254,11 @@ def dropin_counters() -> dict:
     a, b = C.c_uint64(), C.c_uint64()
     check(lib().rick_dropin_counters(C.byref(a), C.byref(b)), "rick_dropin_counters")
     return {"plans_created": int(a.value), "row_allocations": int(b.value)}
+
+
+def dropin_release() -> None:
+    """Frees the drop-ins' cached plans and buffers on every device."""
+    check(lib().rick_dropin_release(), "rick_dropin_release")
 
 
 def fft_planes(grid, num_w_planes, grid_size_x, grid_size_y, out=None):

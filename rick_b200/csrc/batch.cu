@@ -382,7 +382,8 @@ int time_runs(rick_batch *b, int reps, float *ms) {
 }
 
 // Coordinate descent over the gridder's records per work item, its blocks per
-// SM and the column pass's planes in flight (FP32 only), timing the batch.
+// SM and the column pass's form (state in tensor memory, or planes in flight),
+// timing the batch.
 int autotune(rick_batch *b) {
   TuneKey key;
   key.precision = b->precision;
@@ -399,7 +400,7 @@ int autotune(rick_batch *b) {
       return RICK_OK;
     }
   }
-  rick_batch_tuning best{2048, 6, b->precision == RICK_PREC_FP64 ? 1 : 2};
+  rick_batch_tuning best{2048, 6, 0};
   b->tune = best;
   float best_ms = 0.f;
   RICK_TRY(time_runs(b, 2, &best_ms));
@@ -423,9 +424,12 @@ int autotune(rick_batch *b) {
     t.grid_blocks_per_sm = bps;
     RICK_TRY(trial(t));
   }
-  if (b->precision == RICK_PREC_MIXED) {
+  // the column pass: state in tensor memory (0), or in registers with one or
+  // (mixed form) two planes per iteration
+  for (int pif : {1, 2}) {
+    if (pif == 2 && b->precision != RICK_PREC_MIXED) continue;
     rick_batch_tuning t = best;
-    t.planes_in_flight = 1;
+    t.planes_in_flight = pif;
     RICK_TRY(trial(t));
   }
   b->tune = best;
@@ -546,7 +550,7 @@ int rick_batch_create(rick_batch **out, const rick_job_desc *jobs, int njobs, in
     b->tune = *tuning;
     if (b->tune.max_chunk < 64) b->tune.max_chunk = 64;
     if (b->tune.grid_blocks_per_sm < 1) b->tune.grid_blocks_per_sm = 1;
-    if (b->tune.planes_in_flight < 1) b->tune.planes_in_flight = 1;
+    if (b->tune.planes_in_flight < 0 || b->tune.planes_in_flight > 2) b->tune.planes_in_flight = 0;
   } else {
     st = autotune(b);
   }

@@ -208,7 +208,7 @@ __global__ void k_item_count(const uint32_t *__restrict__ bin_off, uint64_t nbin
 // G lanes reduces one row's samples with 16-byte loads (V4) or scalar loads;
 // after G rounds every lane holds the sum of "its" row, and the records are
 // scattered one row per lane with warp-combined cursor increments.
-template <int G, bool V4>
+template <int G, bool V4, bool SHARD>
 __device__ __forceinline__ void scatter_rows(
     const double *__restrict__ uu, const double *__restrict__ vv, const double *__restrict__ ww,
     const float *__restrict__ weight, const float *__restrict__ vis_re,
@@ -220,17 +220,20 @@ __device__ __forceinline__ void scatter_rows(
   const unsigned lane = lane_id();
   const unsigned sub = lane % G, grp = lane / G;
   const uint64_t nv = (uint64_t)nchan * npol;
-  // where the lane's own row goes, before any sample is read: rows that reach
-  // no tile (dropped, outside the sector, of another shard's planes, or with
-  // the footprint off the grid) never stream their samples
-  const uint64_t i_own = base + lane;
-  RowPos p;
-  p.keep = false;
-  p.other = false;
-  if (i_own < nrows) p = row_position(uu[i_own], vv[i_own], ww[i_own], g);
-  uint32_t bins[4];
-  footprint_bins(p, g, bins);
-  const bool need = bins[0] != kNoBin;
+  // A w-plane shard (SHARD) holds a fraction of the rows: its rows of other
+  // planes (and rows that reach no tile) are found before any sample is read,
+  // so they never stream their samples.  A whole-cube plan keeps nearly every
+  // row and compiles without the check.
+  bool need = true;
+  if (SHARD) {
+    const uint64_t i_own = base + lane;
+    RowPos q;
+    q.keep = false;
+    if (i_own < nrows) q = row_position(uu[i_own], vv[i_own], ww[i_own], g);
+    uint32_t qb[4];
+    footprint_bins(q, g, qb);
+    need = qb[0] != kNoBin;
+  }
   double my_re = 0.0, my_im = 0.0;
 #pragma unroll 1
   for (int round = 0; round < G; round++) {
@@ -286,6 +289,12 @@ __device__ __forceinline__ void scatter_rows(
     }
   }
 
+  const uint64_t i = base + lane;
+  RowPos p;
+  p.keep = false;
+  if (i < nrows) p = row_position(uu[i], vv[i], ww[i], g);
+  uint32_t bins[4];
+  footprint_bins(p, g, bins);
   offset_bins(bins, bin_base);
   gridded += p.keep ? 1u : 0u;
   RecF64 r;
@@ -320,7 +329,7 @@ __device__ __forceinline__ void add_scatter_counts(uint32_t gridded, uint32_t nr
   }
 }
 
-template <int G, bool V4>
+template <int G, bool V4, bool SHARD>
 __global__ void __launch_bounds__(256)
     k_bin_scatter(const double *__restrict__ uu, const double *__restrict__ vv,
                   const double *__restrict__ ww, const float *__restrict__ weight,
@@ -332,8 +341,8 @@ __global__ void __launch_bounds__(256)
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
   uint32_t gridded = 0, nrec = 0;
   for (uint64_t base = warp * 32; base < nrows; base += nwarps * 32)
-    scatter_rows<G, V4>(uu, vv, ww, weight, vis_re, vis_im, nrows, nchan, npol, g, base, 0,
-                        bin_off, bin_cursor, rec, gridded, nrec);
+    scatter_rows<G, V4, SHARD>(uu, vv, ww, weight, vis_re, vis_im, nrows, nchan, npol, g, base,
+                               0, bin_off, bin_cursor, rec, gridded, nrec);
   add_scatter_counts(gridded, nrec, counters);
 }
 
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(256, 3)
     const int k = lo + batch_job_of(sc_units + lo, hi - lo, u);
     const BatchJob &J = jobs[sc_jobs[k]];
     const Geometry g = J.g;
-    scatter_rows<G, V4>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan, J.npol,
+    scatter_rows<G, V4, false>(J.uu, J.vv, J.ww, J.weight, J.vis_re, J.vis_im, J.nrows, J.nchan, J.npol,
                         g, (u - sc_units[k]) * 32, J.bin_base, bin_off, bin_cursor, rec, gridded,
                         nrec);
   }
@@ -369,9 +378,14 @@ void launch_scatter(int blocks, cudaStream_t st, const double *uu, const double 
                     const float *vis_im, uint64_t nrows, uint32_t nchan, uint32_t npol,
                     const Geometry &g, Scratch &s) {
   RICK_LAUNCHED();
-  k_bin_scatter<G, V4><<<blocks, 256, 0, st>>>(uu, vv, ww, weight, vis_re, vis_im, nrows, nchan,
-                                               npol, g, s.bin_count, s.bin_cursor, s.records,
-                                               s.counters);
+  if (g.nw_total > 0 && g.nw_total != g.nw)
+    k_bin_scatter<G, V4, true><<<blocks, 256, 0, st>>>(uu, vv, ww, weight, vis_re, vis_im, nrows,
+                                                       nchan, npol, g, s.bin_count, s.bin_cursor,
+                                                       s.records, s.counters);
+  else
+    k_bin_scatter<G, V4, false><<<blocks, 256, 0, st>>>(uu, vv, ww, weight, vis_re, vis_im, nrows,
+                                                        nchan, npol, g, s.bin_count, s.bin_cursor,
+                                                        s.records, s.counters);
 }
 
 }  // namespace

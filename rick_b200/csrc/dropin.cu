@@ -295,6 +295,27 @@ int rick_set_device(int device) {
 
 int rick_last_status(void) { return g_last_status; }
 
+int rick_dropin_release(void) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (int dev = 0; dev < kMaxDevices; dev++) {
+    RowBufs &b = g_rows[dev];
+    if (!g_plans[dev] && !g_dimg[dev] && !b.uvw && !b.wt && !b.vr && !b.vi) continue;
+    RICK_CUDA(cudaSetDevice(dev));
+    if (g_plans[dev]) rick_plan_destroy(g_plans[dev]);
+    g_plans[dev] = nullptr;
+    if (g_dimg[dev]) cudaFree(g_dimg[dev]);
+    g_dimg[dev] = nullptr;
+    g_dimg_vals[dev] = 0;
+    for (void *p : {(void *)b.uvw, (void *)b.wt, (void *)b.vr, (void *)b.vi})
+      if (p) cudaFree(p);
+    b = RowBufs{};
+  }
+  cudaSetDevice(prev);
+  return RICK_OK;
+}
+
 int rick_dropin_counters(uint64_t *plans_created, uint64_t *row_allocations) {
   std::lock_guard<std::mutex> lock(g_mu);
   if (plans_created) *plans_created = g_plans_created;
@@ -345,7 +366,7 @@ int rick_kernel_names(const char **names, int max_names) {
   static const char *k[] = {"k_bin_count",        "k_item_count",       "k_bin_scatter",
                             "k_scan_block",       "k_scan_add",         "k_grid_tiles",
                             "k_zero_split_tiles", "k_row_list",         "k_fft_units",
-                            "k_fft_rows",         "k_fft_cols_image",   "k_fft_cols_tm",      "k_phase_sum",
+                            "k_fft_rows",         "k_fft_cols_image",   "k_fft_cols_tm",      "k_fft_cols_tm_multi", "k_phase_sum",
                             "k_export_cube",      "k_import_cube",      "k_bin_count_batch",
                             "k_bin_scatter_batch", "k_grid_tiles_batch", "k_zero_split_tiles_batch",
                             "k_fft_rows_multi",   "k_fft_cols_multi",   "k_uvw_init",

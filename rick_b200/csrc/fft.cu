@@ -810,6 +810,30 @@ __device__ __forceinline__ void wait_st8(uint32_t (&r)[8]) {
                : "memory");
 }
 
+__device__ __forceinline__ void ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void wait_ld4(uint32_t (&a)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void st4(uint32_t taddr, const uint32_t (&r)[4]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr),
+               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3])
+               : "memory");
+}
+__device__ __forceinline__ void wait_st4(uint32_t (&r)[4]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])
+               :
+               : "memory");
+}
+
 __device__ __forceinline__ double join(uint32_t lo, uint32_t hi) {
   return __hiloint2double((int)hi, (int)lo);
 }
@@ -825,25 +849,33 @@ __host__ __device__ constexpr uint32_t tm_cols(int threads) {
   return (uint32_t)(threads / 32 / 4) * 64u;
 }
 
-template <int LOGN>
+// Shared memory of the TMEM column pass: NB column buffers per row group and
+// 16 bytes for the TMEM address.
+template <typename T, int LOGN, int NB>
 __host__ __device__ constexpr size_t cols_tm_smem_bytes(int rpc) {
-  return (size_t)rpc * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(double2) + 16;
+  return (size_t)rpc * NB * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(typename V2<T>::t) + 16;
 }
 
-// Columns base..base+rpc-1 of one job (one per row group), FP64.
-// `taddr` is the thread's TMEM address: its lane quarter and its warp's 64
-// columns -- [0, 32) the 8 running sums, [32, 64) the 8 steps, 4 words each
-// (re lo/hi, im lo/hi), pixel q at 4q.
-template <int LOGN>
-__device__ __forceinline__ void fft_col_unit_tm(double2 *s, uint32_t base, const ColJob<double> &J,
-                                                uint32_t taddr) {
+// Columns base..base+rpc-1 of one job (one per row group).  The FFT runs in
+// T (FP64 for the plain form, FP32 for the mixed one); the recurrence, its
+// steps and the anchor factor are FP64 in both, so the mixed form adds no
+// phase error to its FP32 transform's.  NB = 2 double-buffers the column
+// loads (the next plane's copies fly during this plane's transform), NB = 1
+// issues them once the transform has read the buffer (each thread's first
+// FFT pass reads exactly the rows it copied, so that pass needs no barrier
+// after the copies).  `taddr` is the thread's TMEM address: its lane quarter
+// and its warp's 64 columns, 8 per pixel q at 8q -- the running sum (re lo/hi,
+// im lo/hi) then the step -- so one 8-column load brings both.
+template <typename T, int LOGN, int NB>
+__device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t base,
+                                                const ColJob<T> &J, uint32_t taddr) {
   constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
-  constexpr int CB = col_block<double>();
-  using V = double2;
+  constexpr int CB = col_block<T>();
+  using V = typename V2<T>::t;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
   const int nx = J.nx, ny = J.ny, nw = J.nw, nty = J.nty;
   const uint32_t *__restrict__ counts = J.counts;
-  V *buf = s + grp * LEN;
+  V *bufs = s + grp * NB * LEN;
   const uint32_t n = base + grp;
   const bool active = n < (uint32_t)nx;
   const bool phase = J.phase_on && J.nw_total > 1;
@@ -852,15 +884,16 @@ __device__ __forceinline__ void fft_col_unit_tm(double2 *s, uint32_t base, const
     do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
     return iw;
   };
-  // the touched rows of plane iw into the buffer (untouched rows zero-filled)
-  auto load_plane = [&](int iw) {
+  // the touched rows of plane iw into buffer b (untouched rows zero-filled)
+  auto load_plane = [&](int iw, int b) {
     const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
-    const V *col = J.cube + blocked_index<double>(iw, 0, active ? n : 0, nx, ny);
+    const V *col = J.cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);
+    V *buf = bufs + b * LEN;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int k = t + q * G;
       const bool touched = active && ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u);
-      cp_async_zfill<double>(buf + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
+      cp_async_zfill<T>(buf + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
     }
     cp_async_commit();
   };
@@ -871,118 +904,110 @@ __device__ __forceinline__ void fft_col_unit_tm(double2 *s, uint32_t base, const
     return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
   };
   int iw = prev_plane(nw);
-  if (iw >= 0) load_plane(iw);
+  int cur = 0;  // buffer of plane iw
+  if (iw >= 0) load_plane(iw, cur);
   // the per-pixel steps into TMEM
   const double dwstep = __dmul_rn(twopi, J.dw);
 #pragma unroll
-  for (int h = 0; h < kVpt / 2; h++) {
-    uint32_t w8[8];
-#pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int m = t + (2 * h + e) * G;
-      double sn = 0.0, cs = 1.0;
-      if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(m), 1.0)), &sn, &cs);
-      tm::split(cs, w8[4 * e + 0], w8[4 * e + 1]);
-      tm::split(sn, w8[4 * e + 2], w8[4 * e + 3]);
-    }
-    tm::st8(taddr + 32 + 8 * h, w8);
-    tm::wait_st8(w8);
+  for (int q = 0; q < kVpt; q++) {
+    const int m = t + q * G;
+    double sn = 0.0, cs = 1.0;
+    if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(m), 1.0)), &sn, &cs);
+    uint32_t w4[4];
+    tm::split(cs, w4[0], w4[1]);
+    tm::split(sn, w4[2], w4[3]);
+    tm::st4(taddr + 8 * q + 4, w4);
+    tm::wait_st4(w4);
   }
   bool first = true;
   int prev = iw;
   while (iw >= 0) {
     cp_async_wait<0>();
-    __syncthreads();  // the plane's copies have landed in every thread's rows
-    Cx<double> x[kVpt];
-    fft_to_regs<double, LOGN>(buf, t, J.tw, x);
-    __syncthreads();  // every thread has read the buffer
+    if (NB == 2) __syncthreads();  // every copy has landed; the other buffer is free
     const int nxt = prev_plane(iw);
-    if (nxt >= 0) load_plane(nxt);
+    if (NB == 2 && nxt >= 0) load_plane(nxt, cur ^ 1);
+    Cx<T> x[kVpt];
+    fft_to_regs<T, LOGN>(bufs + cur * LEN, t, J.tw, x);
+    if (NB == 1) {
+      __syncthreads();  // every thread has read the buffer
+      if (nxt >= 0) load_plane(nxt, cur);
+    }
     const int gap = prev - iw;
 #pragma unroll
-    for (int h = 0; h < kVpt / 2; h++) {
-      uint32_t a8[8], s8[8];
+    for (int q = 0; q < kVpt; q++) {
+      uint32_t a4[4];
       if (first) {
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          tm::split(x[2 * h + e].re, a8[4 * e + 0], a8[4 * e + 1]);
-          tm::split(x[2 * h + e].im, a8[4 * e + 2], a8[4 * e + 3]);
-        }
+        tm::split((double)x[q].re, a4[0], a4[1]);
+        tm::split((double)x[q].im, a4[2], a4[3]);
       } else {
-        tm::ld8(taddr + 8 * h, a8);
-        tm::ld8(taddr + 32 + 8 * h, s8);
-        tm::wait_ld8(a8, s8);
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          double ar = tm::join(a8[4 * e + 0], a8[4 * e + 1]);
-          double ai = tm::join(a8[4 * e + 2], a8[4 * e + 3]);
-          const double sr = tm::join(s8[4 * e + 0], s8[4 * e + 1]);
-          const double si = tm::join(s8[4 * e + 2], s8[4 * e + 3]);
-          for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
-            const double tr = fma(ar, sr, -ai * si);
-            ai = fma(ar, si, ai * sr);
-            ar = tr;
-          }
-          const double nr = fma(ar, sr, fma(-ai, si, x[2 * h + e].re));
-          const double ni = fma(ar, si, fma(ai, sr, x[2 * h + e].im));
-          tm::split(nr, a8[4 * e + 0], a8[4 * e + 1]);
-          tm::split(ni, a8[4 * e + 2], a8[4 * e + 3]);
+        uint32_t r8[8];
+        tm::ld8(taddr + 8 * q, r8);
+        tm::wait_ld8(r8);
+        double ar = tm::join(r8[0], r8[1]);
+        double ai = tm::join(r8[2], r8[3]);
+        const double sr = tm::join(r8[4], r8[5]);
+        const double si = tm::join(r8[6], r8[7]);
+        for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
+          const double tr = fma(ar, sr, -ai * si);
+          ai = fma(ar, si, ai * sr);
+          ar = tr;
         }
+        const double nr = fma(ar, sr, fma(-ai, si, (double)x[q].re));
+        const double ni = fma(ar, si, fma(ai, sr, (double)x[q].im));
+        tm::split(nr, a4[0], a4[1]);
+        tm::split(ni, a4[2], a4[3]);
       }
-      tm::st8(taddr + 8 * h, a8);
-      tm::wait_st8(a8);
+      tm::st4(taddr + 8 * q, a4);
+      tm::wait_st4(a4);
     }
     first = false;
     prev = iw;
     iw = nxt;
+    if (NB == 2) cur ^= 1;
   }
   // image = norm * P * sum, P the factor of the lowest plane with data
   const double cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + prev), J.dw)));
 #pragma unroll
-  for (int h = 0; h < kVpt / 2; h++) {
-    uint32_t a8[8];
+  for (int q = 0; q < kVpt; q++) {
+    const int m = t + q * G;
+    double re = 0.0, im = 0.0;
     if (!first) {
-      tm::ld8(taddr + 8 * h, a8);
-      tm::wait_ld8(a8);
+      uint32_t a4[4];
+      tm::ld4(taddr + 8 * q, a4);
+      tm::wait_ld4(a4);
+      const double ar = tm::join(a4[0], a4[1]);
+      const double ai = tm::join(a4[2], a4[3]);
+      double pr = 1.0, pi = 0.0;
+      if (phase) {
+        const double root = root_of(m);
+        double sn, cs;
+        sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+        const double amp = J.dwnorm * root;
+        pr = cs * amp;
+        pi = sn * amp;
+      }
+      re = J.norm * fma(ar, pr, -ai * pi);
+      im = J.norm * fma(ar, pi, ai * pr);
     }
-#pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int m = t + (2 * h + e) * G;
-      double re = 0.0, im = 0.0;
-      if (!first) {
-        const double ar = tm::join(a8[4 * e + 0], a8[4 * e + 1]);
-        const double ai = tm::join(a8[4 * e + 2], a8[4 * e + 3]);
-        double pr = 1.0, pi = 0.0;
-        if (phase) {
-          const double root = root_of(m);
-          double sn, cs;
-          sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
-          const double amp = J.dwnorm * root;
-          pr = cs * amp;
-          pi = sn * amp;
-        }
-        re = J.norm * fma(ar, pr, -ai * pi);
-        im = J.norm * fma(ar, pi, ai * pr);
-      }
-      if (active) {
-        J.img_re[(uint64_t)m * nx + n] = re;
-        J.img_im[(uint64_t)m * nx + n] = im;
-      }
+    if (active) {
+      J.img_re[(uint64_t)m * nx + n] = re;
+      J.img_im[(uint64_t)m * nx + n] = im;
     }
   }
 }
 
 template <int LOGN> constexpr int tm_min_blocks() { return 1024 / block_threads<LOGN>(); }
 
-template <int LOGN>
+template <typename T, int LOGN, int NB>
 __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
-    k_fft_cols_tm(ColJob<double> J) {
+    k_fft_cols_tm(ColJob<T> J) {
   constexpr int G = (1 << LOGN) / kVpt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto *s = reinterpret_cast<double2 *>(smem_raw);
+  auto *s = reinterpret_cast<typename V2<T>::t *>(smem_raw);
   const int rpc = blockDim.x / G;
   // the TMEM address slot sits after the column buffers
-  uint32_t *slot = reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<LOGN>(rpc) - 16);
+  uint32_t *slot =
+      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN, NB>(rpc) - 16);
   constexpr uint32_t ncols = tm_cols(block_threads<LOGN>());
   const int warp = threadIdx.x / 32;
   if (warp == 0) {
@@ -995,8 +1020,69 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
   const uint32_t tbase = *slot;
   const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 64u;
   for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)J.nx; base += gridDim.x * rpc) {
-    fft_col_unit_tm<LOGN>(s, base, J, taddr);
+    fft_col_unit_tm<T, LOGN, NB>(s, base, J, taddr);
     __syncthreads();  // the column buffers are rewritten for the next columns
+  }
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    tm::dealloc(tbase, ncols);
+  }
+}
+
+// The TMEM column pass over the jobs col_jobs[lo..hi-1] of a batch (all of FFT
+// length 2^LOGN along y): the column groups of the k-th listed job are
+// col_units[k] .. col_units[k+1]-1.
+template <typename T, int LOGN, int NB>
+__global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
+    k_fft_cols_tm_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
+                        int lo, int hi, const uint32_t *__restrict__ col_units,
+                        const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts) {
+  constexpr int G = (1 << LOGN) / kVpt;
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto *s = reinterpret_cast<V *>(smem_raw);
+  const int rpc = blockDim.x / G;
+  uint32_t *slot =
+      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN, NB>(rpc) - 16);
+  constexpr uint32_t ncols = tm_cols(block_threads<LOGN>());
+  const int warp = threadIdx.x / 32;
+  if (warp == 0) {
+    tm::alloc(slot, ncols);
+    tm::relinquish();
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 64u;
+  const uint32_t u1 = col_units[hi];
+  for (uint32_t u = col_units[lo] + blockIdx.x; u < u1; u += gridDim.x) {
+    const int k = lo + batch_job_of(col_units + lo, hi - lo, u);
+    const BatchJob &B = jobs[col_jobs[k]];
+    ColJob<T> J;
+    J.cube = (const V *)B.blocked;
+    J.nx = B.g.nx;
+    J.ny = B.g.ny;
+    J.nw = B.g.nw;
+    J.nty = B.g.nty;
+    J.w_first = B.g.w_first;
+    J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
+    J.rowmask = rowmask + B.mask_base;
+    J.counts = counts + B.counts_base;
+    J.tw = (const V *)B.tw_y;
+    J.ltab = B.ltab;
+    J.mtab = B.mtab;
+    J.wmin = B.wmin;
+    J.dw = B.dw_phase;
+    J.dwnorm = B.dwnorm;
+    J.norm = B.norm;
+    J.phase_on = B.phase_on;
+    J.img_re = B.img_re;
+    J.img_im = B.img_im;
+    fft_col_unit_tm<T, LOGN, NB>(s, (u - col_units[k]) * (uint32_t)rpc, J, taddr);
+    __syncthreads();
   }
   tm::fence_before();
   __syncthreads();
@@ -1211,45 +1297,81 @@ int launch_cols_impl(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
-// One job's FP64 column pass with the per-pixel state in TMEM.  The dynamic
-// shared memory is padded so that shared memory, not the TMEM allocation,
-// bounds the blocks per SM at 512 / (columns a block allocates): a further
-// block could not allocate and would wait for one of the others to finish.
-template <int LOGN>
-int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
+// Implementation choices of the column pass, for measurements: RICK_COLS_TMEM=0
+// selects the register-resident kernels, RICK_COLS_TMEM_DB=0 single buffers.
+bool env_on(const char *name) {
+  const char *e = getenv(name);
+  return !(e && e[0] == '0');
+}
+bool cols_tm_enabled() {
+  static const bool on = env_on("RICK_COLS_TMEM");
+  return on;
+}
+bool cols_tm_db_allowed() {
+  static const bool on = env_on("RICK_COLS_TMEM_DB");
+  return on;
+}
+
+// One job's column pass with the per-pixel state in TMEM.  The dynamic shared
+// memory is padded so that shared memory, not the TMEM allocation, bounds the
+// blocks per SM at 512 / (columns a block allocates): a further block could
+// not allocate and would wait for one of the others to finish.  Column loads
+// are double-buffered when two buffers per block fit beside the other blocks.
+template <typename T, int LOGN, int NB>
+int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int smem_sm,
+                      int reserved) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
   const int rpc = BT / G;
   const int max_blocks = (int)(512u / tm_cols(BT));
-  int dev = 0, smem_sm = 0, reserved = 0;
-  RICK_CUDA(cudaGetDevice(&dev));
-  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-  size_t sm = cols_tm_smem_bytes<LOGN>(rpc);
+  size_t sm = cols_tm_smem_bytes<T, LOGN, NB>(rpc);
   const size_t floor_b = (size_t)smem_sm / (size_t)(max_blocks + 1) + 1;
   if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
   sm = (sm + 15) & ~(size_t)15;
-  RICK_CUDA(cudaFuncSetAttribute(k_fft_cols_tm<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm));
-  int per_sm = 0;
-  RICK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_cols_tm<LOGN>, BT, sm));
-  per_sm = std::min(std::max(per_sm, 1), max_blocks);
+  // the whole shared memory as carveout: with the driver's default choice
+  // (164 KB for 77 KB blocks) the SM held one 4096-point block, not two
+  const void *fn = f.one ? (const void *)k_fft_cols_tm<T, LOGN, NB>
+                         : (const void *)k_fft_cols_tm_multi<T, LOGN, NB>;
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+  // blocks per SM from the kernel's own needs: registers, shared memory, threads
+  cudaFuncAttributes fa{};
+  RICK_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const int regs_per_warp = ((std::max(fa.numRegs, 1) * 32 + 255) / 256) * 256;
+  const int by_regs = 65536 / (regs_per_warp * (BT / 32));
+  const int by_smem = (int)((size_t)smem_sm / (sm + (size_t)reserved));
+  const int by_threads = 2048 / BT;
+  const int per_sm = std::max(1, std::min({max_blocks, by_regs, by_smem, by_threads}));
   const int blocks = (int)std::min<uint64_t>(std::max<uint32_t>(c.units, 1),
                                              (uint64_t)num_sms() * per_sm);
-  ColJob<double> J = col_job<double>(*f.one, f);
-  // the slot of the TMEM address sits in the last 16 bytes of the unpadded layout
   RICK_LAUNCHED();
-  k_fft_cols_tm<LOGN><<<blocks, BT, sm, st>>>(J);
+  if (f.one) {
+    k_fft_cols_tm<T, LOGN, NB><<<blocks, BT, sm, st>>>(col_job<T>(*f.one, f));
+  } else {
+    k_fft_cols_tm_multi<T, LOGN, NB><<<blocks, BT, sm, st>>>(f.jobs, f.col_jobs, c.lo, c.hi,
+                                                             f.col_units, f.rowmask, f.counts);
+  }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
 
-bool cols_tm_enabled() {
-  static const bool on = [] {
-    const char *e = getenv("RICK_COLS_TMEM");
-    return !(e && e[0] == '0');
-  }();
-  return on;
+template <typename T, int LOGN>
+int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
+  constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
+  const int rpc = BT / G;
+  const int max_blocks = (int)(512u / tm_cols(BT));
+  int dev = 0, smem_sm = 0, reserved = 0, smem_block = 0;
+  RICK_CUDA(cudaGetDevice(&dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t two = cols_tm_smem_bytes<T, LOGN, 2>(rpc);
+  if (cols_tm_db_allowed() && two <= (size_t)smem_block &&
+      (two + (size_t)reserved) * (size_t)max_blocks <= (size_t)smem_sm)
+    return launch_cols_tm_nb<T, LOGN, 2>(f, c, st, smem_sm, reserved);
+  return launch_cols_tm_nb<T, LOGN, 1>(f, c, st, smem_sm, reserved);
 }
+
 
 template <typename T, int LOGN>
 int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
@@ -1258,8 +1380,11 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   // in order of preference, the first that fits: two planes per iteration
   // (FP32), double-buffered loads, the per-pixel phase steps
   constexpr size_t kMax = 220 * 1024;
-  if constexpr (sizeof(T) == 8) {
-    if (f.one && cols_tm_enabled()) return launch_cols_tm<LOGN>(f, c, st);
+  // the TMEM-state pass: always for one job; for a batch when its schedule
+  // asks for it (planes in flight 0) and the length is a batch length
+  if (cols_tm_enabled() && f.one) return launch_cols_tm<T, LOGN>(f, c, st);
+  if constexpr (LOGN <= kMultiMaxLog) {
+    if (cols_tm_enabled() && !f.one && f.cols_pp == 0) return launch_cols_tm<T, LOGN>(f, c, st);
   }
 #define RICK_TRY_COLS(DB, RC, PP)                            \
   if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)           \

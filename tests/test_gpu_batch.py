@@ -100,7 +100,7 @@ def test_batch_matches_oracle(precision):
         assert st["rows_gridded"] + st["rows_dropped"] == st["rows_in"]
         t = b.tuning()
         assert t["max_chunk"] >= 64 and t["grid_blocks_per_sm"] >= 1
-        assert t["planes_in_flight"] in (1, 2)
+        assert t["planes_in_flight"] in (0, 1, 2)   # 0: column-pass state in tensor memory
 
 
 def test_batch_equals_plans_alone():
