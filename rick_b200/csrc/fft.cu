@@ -252,6 +252,71 @@ __device__ __forceinline__ void fft_to_regs(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
+// The first pass (stride 1, radix 8) of a transform whose thread t holds only
+// some of its inputs: thread t's butterfly reads rows t + r*N/8, r = 0..7 --
+// exactly the rows it copied in -- and bit r of `rows8` says whether row
+// t + r*N/8 was copied; the other rows are zeros that are never read.
+template <typename T, int N>
+__device__ __forceinline__ void stockham_first_pass_m(typename V2<T>::t *s, int t,
+                                                      uint32_t rows8) {
+  constexpr int G = N / kVpt;
+  Cx<T> v[8];
+#pragma unroll
+  for (int r = 0; r < 8; r++)
+    v[r] = ((rows8 >> r) & 1u) ? lds<T>(s, t + r * G) : Cx<T>{(T)0, (T)0};
+  __syncthreads();
+  Dft<T, 8>::run(v);
+#pragma unroll
+  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
+  __syncthreads();
+}
+
+// fft_to_regs with the first pass reading only the rows of `rows8`.
+template <typename T, int LOGN>
+__device__ __forceinline__ void fft_to_regs_m(typename V2<T>::t *s, int t,
+                                              const typename V2<T>::t *__restrict__ tw,
+                                              Cx<T> out[kVpt], uint32_t rows8) {
+  constexpr int N = 1 << LOGN;
+  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+  constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
+  constexpr int NPASS = P8 + (REM ? 1 : 0);
+  static_assert(NPASS >= 2, "the first pass is a radix-8 pass before the last one");
+  stockham_first_pass_m<T, N>(s, t, rows8);
+  int Ns = 8;
+#pragma unroll
+  for (int p = 1; p < NPASS - 1; p++) {
+    stockham_pass<T, N, 8>(s, t, Ns, tw);
+    Ns *= 8;
+  }
+  stockham_last_pass<T, N, LASTR>(s, t, tw, out);
+}
+
+// fft_to_regs with the first pass fed from registers: v[r] is thread t's input
+// at t + r*N/8 (the inputs of its first-pass butterfly), so nothing is stored
+// to shared memory before that butterfly.  The buffer must be free (no thread
+// still reading it) when this is called.
+template <typename T, int LOGN>
+__device__ __forceinline__ void fft_to_regs_r(typename V2<T>::t *s, int t,
+                                              const typename V2<T>::t *__restrict__ tw,
+                                              Cx<T> v[8], Cx<T> out[kVpt]) {
+  constexpr int N = 1 << LOGN;
+  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+  constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
+  constexpr int NPASS = P8 + (REM ? 1 : 0);
+  static_assert(NPASS >= 2, "the first pass is a radix-8 pass before the last one");
+  Dft<T, 8>::run(v);
+#pragma unroll
+  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
+  __syncthreads();
+  int Ns = 8;
+#pragma unroll
+  for (int p = 1; p < NPASS - 1; p++) {
+    stockham_pass<T, N, 8>(s, t, Ns, tw);
+    Ns *= 8;
+  }
+  stockham_last_pass<T, N, LASTR>(s, t, tw, out);
+}
+
 // PP transforms at once, one per shared buffer, sharing every barrier (twice
 // the independent work between barriers for PP = 2).
 template <typename T, int N, int R, int PP>
@@ -393,6 +458,8 @@ __device__ __forceinline__ void fft_row_unit(typename V2<T>::t *s, bool active, 
   if (!active) w = k = 0;
   const uint32_t *tm = tilemask + ((uint64_t)w * nty + (k >> 5)) * tmw;
   const uint64_t rowbase = ((uint64_t)w * ny + k) * nx;
+  // thread t's inputs x = t + q*G are its first butterfly's: straight to registers
+  Cx<T> in[kVpt];
 #pragma unroll
   for (int q = 0; q < kVpt; q++) {
     const int x = t + q * G;
@@ -400,11 +467,10 @@ __device__ __forceinline__ void fft_row_unit(typename V2<T>::t *s, bool active, 
     v.x = 0;
     v.y = 0;
     if (active && ((tm[x >> 10] >> ((x >> 5) & 31)) & 1u)) v = cube[rowbase + x];
-    srow[pad(x)] = v;
+    in[q] = {v.x, v.y};
   }
-  __syncthreads();
   Cx<T> res[kVpt];
-  fft_to_regs<T, LOGN>(srow, t, tw, res);
+  fft_to_regs_r<T, LOGN>(srow, t, tw, in, res);
   if (active) {
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
@@ -731,9 +797,11 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
 // and its step s -- and the phase needs one sincos per pixel for s and one
 // for P per column, none per plane.  The reference evaluates every plane's
 // factor with its own sincos (phase_correction.cu:205-226); the recurrence's
-// products move each factor by a few ulp per plane (< 1e-13 relative over 64
-// planes of a 8192^2 wide-field image), below the rounding of the reference's
-// own phase argument.
+// products move each factor by a few ulp per plane.  Modelled in long double
+// for the worst pixels: 8.4e-14 at 4096^2 x 32 planes (w from -7.5e3 to 7.8e3
+// wavelengths) and 2.6e-13 at 8192^2 x 64 planes (w to 1.1e5), below the
+// rounding of the reference's own per-plane phase argument there (1.3e-13 and
+// 3.3e-13 at the image corner).
 //
 // The two complex values of the thread's 8 pixels (64 32-bit words) live in
 // tensor memory (TMEM, 512 columns x 128 lanes of 32 bits per SM), not in
@@ -767,8 +835,6 @@ __device__ __forceinline__ void fence_before() {
 __device__ __forceinline__ void fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 }
-__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
-__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 // 8 consecutive columns of the thread's lane; the registers are ready after
 // wait_ld8, which names them so that no use moves above the wait.
@@ -779,14 +845,6 @@ __device__ __forceinline__ void ld8(uint32_t taddr, uint32_t (&r)[8]) {
                : "r"(taddr)
                : "memory");
 }
-__device__ __forceinline__ void wait_ld8(uint32_t (&a)[8], uint32_t (&b)[8]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
-               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
-                 "+r"(a[6]), "+r"(a[7]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]),
-                 "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7])
-               :
-               : "memory");
-}
 __device__ __forceinline__ void wait_ld8(uint32_t (&a)[8]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n"
                : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
@@ -794,22 +852,8 @@ __device__ __forceinline__ void wait_ld8(uint32_t (&a)[8]) {
                :
                : "memory");
 }
-__device__ __forceinline__ void st8(uint32_t taddr, const uint32_t (&r)[8]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(
-                   taddr),
-               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
-               "r"(r[7])
-               : "memory");
-}
-// The stored registers stay untouched until the store has completed.
-__device__ __forceinline__ void wait_st8(uint32_t (&r)[8]) {
-  asm volatile("tcgen05.wait::st.sync.aligned;\n"
-               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
-                 "+r"(r[6]), "+r"(r[7])
-               :
-               : "memory");
-}
 
+// 4 consecutive columns; the registers are ready after wait_ld4.
 __device__ __forceinline__ void ld4(uint32_t taddr, uint32_t (&r)[4]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];\n"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
@@ -827,6 +871,7 @@ __device__ __forceinline__ void st4(uint32_t taddr, const uint32_t (&r)[4]) {
                "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3])
                : "memory");
 }
+// The stored registers stay untouched until the store has completed.
 __device__ __forceinline__ void wait_st4(uint32_t (&r)[4]) {
   asm volatile("tcgen05.wait::st.sync.aligned;\n"
                : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])
@@ -884,18 +929,22 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
     return iw;
   };
-  // the touched rows of plane iw into buffer b (untouched rows zero-filled)
+  // the touched rows of plane iw into buffer b; the untouched ones are left
+  // alone (bit q of the returned mask clear: the first pass reads zero there)
   auto load_plane = [&](int iw, int b) {
     const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
     const V *col = J.cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);
     V *buf = bufs + b * LEN;
+    uint32_t rows8 = 0;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int k = t + q * G;
       const bool touched = active && ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u);
-      cp_async_zfill<T>(buf + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
+      if (touched) cp_async_zfill<T>(buf + pad(k), col + (uint64_t)k * CB, true);
+      rows8 |= (touched ? 1u : 0u) << q;
     }
     cp_async_commit();
+    return rows8;
   };
   // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits
   const double l = active ? J.ltab[n] : 0.0;
@@ -905,7 +954,8 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
   };
   int iw = prev_plane(nw);
   int cur = 0;  // buffer of plane iw
-  if (iw >= 0) load_plane(iw, cur);
+  uint32_t rows8 = 0, rows8_next = 0;  // rows of plane iw (of the next plane) copied
+  if (iw >= 0) rows8 = load_plane(iw, cur);
   // the per-pixel steps into TMEM
   const double dwstep = __dmul_rn(twopi, J.dw);
 #pragma unroll
@@ -925,13 +975,14 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     cp_async_wait<0>();
     if (NB == 2) __syncthreads();  // every copy has landed; the other buffer is free
     const int nxt = prev_plane(iw);
-    if (NB == 2 && nxt >= 0) load_plane(nxt, cur ^ 1);
+    if (NB == 2 && nxt >= 0) rows8_next = load_plane(nxt, cur ^ 1);
     Cx<T> x[kVpt];
-    fft_to_regs<T, LOGN>(bufs + cur * LEN, t, J.tw, x);
+    fft_to_regs_m<T, LOGN>(bufs + cur * LEN, t, J.tw, x, rows8);
     if (NB == 1) {
       __syncthreads();  // every thread has read the buffer
-      if (nxt >= 0) load_plane(nxt, cur);
+      if (nxt >= 0) rows8_next = load_plane(nxt, cur);
     }
+    rows8 = rows8_next;
     const int gap = prev - iw;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
@@ -1297,18 +1348,14 @@ int launch_cols_impl(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
-// Implementation choices of the column pass, for measurements: RICK_COLS_TMEM=0
-// selects the register-resident kernels, RICK_COLS_TMEM_DB=0 single buffers.
+// Implementation choice of the column pass, for measurements: RICK_COLS_TMEM=0
+// selects the register-resident kernels.
 bool env_on(const char *name) {
   const char *e = getenv(name);
   return !(e && e[0] == '0');
 }
 bool cols_tm_enabled() {
   static const bool on = env_on("RICK_COLS_TMEM");
-  return on;
-}
-bool cols_tm_db_allowed() {
-  static const bool on = env_on("RICK_COLS_TMEM_DB");
   return on;
 }
 
@@ -1332,8 +1379,6 @@ int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int 
   const void *fn = f.one ? (const void *)k_fft_cols_tm<T, LOGN, NB>
                          : (const void *)k_fft_cols_tm_multi<T, LOGN, NB>;
   RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared));
   // blocks per SM from the kernel's own needs: registers, shared memory, threads
   cudaFuncAttributes fa{};
   RICK_CUDA(cudaFuncGetAttributes(&fa, fn));
@@ -1342,6 +1387,14 @@ int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int 
   const int by_smem = (int)((size_t)smem_sm / (sm + (size_t)reserved));
   const int by_threads = 2048 / BT;
   const int per_sm = std::max(1, std::min({max_blocks, by_regs, by_smem, by_threads}));
+  // a shared-memory carveout just large enough for those blocks: the rest of
+  // the SM's 256 KB stays L1, which holds the FFT's twiddles (with the whole
+  // carveout as shared memory, the mixed form's 8-byte column copies, cached
+  // in L1, evicted them: its column pass ran 3.47 ms at 4096^2 x 32, 3.04 ms
+  // with this carveout)
+  const int pct = (int)std::min<size_t>(
+      100, ((size_t)per_sm * (sm + (size_t)reserved) * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
   const int blocks = (int)std::min<uint64_t>(std::max<uint32_t>(c.units, 1),
                                              (uint64_t)num_sms() * per_sm);
   RICK_LAUNCHED();
@@ -1357,18 +1410,12 @@ int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int 
 
 template <typename T, int LOGN>
 int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
-  constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
-  const int rpc = BT / G;
-  const int max_blocks = (int)(512u / tm_cols(BT));
-  int dev = 0, smem_sm = 0, reserved = 0, smem_block = 0;
+  int dev = 0, smem_sm = 0, reserved = 0;
   RICK_CUDA(cudaGetDevice(&dev));
   RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
   RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-  RICK_CUDA(cudaDeviceGetAttribute(&smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const size_t two = cols_tm_smem_bytes<T, LOGN, 2>(rpc);
-  if (cols_tm_db_allowed() && two <= (size_t)smem_block &&
-      (two + (size_t)reserved) * (size_t)max_blocks <= (size_t)smem_sm)
-    return launch_cols_tm_nb<T, LOGN, 2>(f, c, st, smem_sm, reserved);
+  // single-buffered column loads: where two buffers per block fit (FP32), the
+  // double-buffered form measured slower (3.14 against 3.04 ms at 4096^2 x 32)
   return launch_cols_tm_nb<T, LOGN, 1>(f, c, st, smem_sm, reserved);
 }
 
