@@ -70,7 +70,7 @@ def plan_kernel_name(stage, nx, ny):
     return {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
             "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
             "fft": f"k_fft_rows<double,{lx}>",
-            "phase": f"k_fft_cols_image<double,{ly}>"}.get(stage, stage)
+            "phase": f"k_fft_cols_tm<double,{ly}>"}.get(stage, stage)
 
 
 def fp64_gemm_tflops(dev) -> float:
@@ -393,9 +393,9 @@ def run_ours(args):
                                 for k, v in stage64.items() if v > 0 and alg[k] > 0},
                 "fft_rows": stats64.get("fft_rows", 0)}
     if dom == "phase" and stats64.get("fft_rows", 0):
-        roofline["note"] = ("column FFT + w-correction + plane sum: bound by FP64 issue and "
-                            "shared-memory traffic, not by HBM (fp64_compute gives the compute "
-                            "roofline)")
+        roofline["note"] = ("column FFT + w-correction + plane sum (per-pixel state in tensor "
+                            "memory): bound by FP64 issue, shared-memory traffic and load "
+                            "latency, not by HBM (fp64_compute gives the compute roofline)")
         # algorithmic FP64 flops of the column pass: a radix-2-equivalent 5 N log2 N per
         # column FFT of every plane (all planes hold data here), plus the w-correction's
         # ~10 flops per pixel and plane
@@ -429,10 +429,10 @@ def run_ours(args):
                 "rel_l2": float(torch.linalg.vector_norm(im - ref_t) / torch.linalg.vector_norm(ref_t)),
                 "max_abs_rel_to_peak": float((im - ref_t).abs().max() / ref_t.abs().max())}
         del ref_t
-        if not args.no_dropin and args.workload == "c2":
-            hrows = _host_rows(host if host is not None else rows)
-            dropin = run_dropin(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, ref_img)
-            del hrows
+    if rank == 0 and world == 1 and not args.no_dropin and args.workload == "c2":
+        hrows = _host_rows(host if host is not None else rows)
+        dropin = run_dropin(hrows, nchan, npol, nx, ny, nw, cfg, res, wmin, wmax, ref_img)
+        del hrows
     del host
     line = {
         "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": args.steps,

@@ -4,8 +4,9 @@
 // They keep one cached plan per device (grown when a call needs more capacity)
 // so repeated calls do not re-allocate.  Host buffers cross PCIe on every call,
 // as in the reference's CUDA wstack (w-stacking.cu:338-348, :414) and
-// phase_correction (phase_correction.cu:137-138, :171-173); device-resident
-// callers use the plan API instead.
+// phase_correction (phase_correction.cu:137-138, :171-173) -- through pinned
+// staging buffers filled by a pool of host threads when the caller's memory is
+// pageable (hostcopy.cu); device-resident callers use the plan API instead.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -171,12 +172,12 @@ int do_wstack(int nw, unsigned int npts, unsigned int nchan, unsigned int npol, 
   struct { double *ptr; } duvw{b.uvw};
   struct { float *ptr; } dwt{b.wt}, dvr{b.vr}, dvi{b.vi};
   cudaStream_t st = 0;
-  RICK_CUDA(cudaMemcpyAsync(duvw.ptr, uu, npts * 8ull, cudaMemcpyHostToDevice, st));
-  RICK_CUDA(cudaMemcpyAsync(duvw.ptr + npts, vv, npts * 8ull, cudaMemcpyHostToDevice, st));
-  RICK_CUDA(cudaMemcpyAsync(duvw.ptr + 2ull * npts, ww, npts * 8ull, cudaMemcpyHostToDevice, st));
-  RICK_CUDA(cudaMemcpyAsync(dwt.ptr, wt, (uint64_t)npts * npol * 4, cudaMemcpyHostToDevice, st));
-  RICK_CUDA(cudaMemcpyAsync(dvr.ptr, vr, nv * 4, cudaMemcpyHostToDevice, st));
-  RICK_CUDA(cudaMemcpyAsync(dvi.ptr, vi, nv * 4, cudaMemcpyHostToDevice, st));
+  RICK_TRY(copy_to_device(duvw.ptr, uu, npts * 8ull, st));
+  RICK_TRY(copy_to_device(duvw.ptr + npts, vv, npts * 8ull, st));
+  RICK_TRY(copy_to_device(duvw.ptr + 2ull * npts, ww, npts * 8ull, st));
+  RICK_TRY(copy_to_device(dwt.ptr, wt, (uint64_t)npts * npol * 4, st));
+  RICK_TRY(copy_to_device(dvr.ptr, vr, nv * 4, st));
+  RICK_TRY(copy_to_device(dvi.ptr, vi, nv * 4, st));
   // accumulate semantics (w-stacking.cu:530-532): start from the caller's grid
   RICK_TRY(rick_plan_import_cube(p, grid, 1, st));
   RICK_TRY(rick_internal_plan_mark_raw(p));

@@ -40,9 +40,12 @@ template <typename T>
 __device__ __forceinline__ Cx<T> cadd(Cx<T> a, Cx<T> b) { return {a.re + b.re, a.im + b.im}; }
 template <typename T>
 __device__ __forceinline__ Cx<T> csub(Cx<T> a, Cx<T> b) { return {a.re - b.re, a.im - b.im}; }
+// a * (br + i bi) with two fused multiply-adds: the library is built without
+// FP contraction (the cell assignment and the phase arguments must round as
+// the reference does), so the transforms ask for their FMAs explicitly.
 template <typename T>
 __device__ __forceinline__ Cx<T> cmul(Cx<T> a, T br, T bi) {
-  return {a.re * br - a.im * bi, a.re * bi + a.im * br};
+  return {fma(a.re, br, -(a.im * bi)), fma(a.re, bi, a.im * br)};
 }
 
 // exp(+2 pi i j / 16) applied to a, j = 0..7 known at compile time after unrolling.
@@ -85,13 +88,26 @@ template <typename T> struct Dft<T, 1> {
   __device__ __forceinline__ static void run(Cx<T> *) {}
 };
 
-// Shared-memory index with one pad element every 16: the stride-R stores of
-// the first pass then spread over the banks.
-__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+// Shared-memory position of element i of a transform: an XOR swizzle of the
+// low bits (no padding), chosen so that every access pattern of the passes is
+// free of bank conflicts -- the runs of consecutive elements, the stride-8
+// stores of the first pass and the pairs of 8-element runs 64 apart of the
+// second (checked by counting wavefronts for every pass of every length).  A
+// 16-byte element (FP64 complex) spans 4 banks and 8 lanes share a wavefront:
+// bits 3..5 are folded into bits 0..2.  An 8-byte element (FP32) spans 2 banks
+// and 16 lanes share a wavefront: bits 4..6 into bits 0..3.  (A pad element
+// every 16, the layout this replaces, left 11-20 % more wavefronts.)  The
+// swizzle keeps i within its aligned 8- or 16-element block, so the lower half
+// of a column stays the lower half.
+template <typename T> __host__ __device__ constexpr int padded(int n) { return n; }
+template <typename T> __device__ __forceinline__ int pad(int i) {
+  if (sizeof(typename V2<T>::t) == 16) return i ^ ((i >> 3) & 7);
+  return i ^ (((i >> 4) & 7) | (((i >> 6) & 1) << 3));
+}
 
 template <typename T>
 __device__ __forceinline__ Cx<T> lds(const typename V2<T>::t *s, int i) {
-  const typename V2<T>::t v = s[pad(i)];
+  const typename V2<T>::t v = s[pad<T>(i)];
   return {v.x, v.y};
 }
 template <typename T>
@@ -99,7 +115,7 @@ __device__ __forceinline__ void sts(typename V2<T>::t *s, int i, Cx<T> c) {
   typename V2<T>::t v;
   v.x = c.re;
   v.y = c.im;
-  s[pad(i)] = v;
+  s[pad<T>(i)] = v;
 }
 
 // Asynchronous global->shared copy of one complex value; zero-filled when
@@ -252,36 +268,18 @@ __device__ __forceinline__ void fft_to_regs(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
-// The first pass (stride 1, radix 8) of a transform whose thread t holds only
-// some of its inputs: thread t's butterfly reads rows t + r*N/8, r = 0..7 --
-// exactly the rows it copied in -- and bit r of `rows8` says whether row
-// t + r*N/8 was copied; the other rows are zeros that are never read.
-template <typename T, int N>
-__device__ __forceinline__ void stockham_first_pass_m(typename V2<T>::t *s, int t,
-                                                      uint32_t rows8) {
-  constexpr int G = N / kVpt;
-  Cx<T> v[8];
-#pragma unroll
-  for (int r = 0; r < 8; r++)
-    v[r] = ((rows8 >> r) & 1u) ? lds<T>(s, t + r * G) : Cx<T>{(T)0, (T)0};
-  __syncthreads();
-  Dft<T, 8>::run(v);
-#pragma unroll
-  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
-  __syncthreads();
-}
-
-// fft_to_regs with the first pass reading only the rows of `rows8`.
+// The passes of an N = 2^LOGN transform after its first (stride-1, radix-8)
+// pass, whose outputs are in shared memory; the last pass leaves its results
+// in registers (out[q] = value at t + q*G).
 template <typename T, int LOGN>
-__device__ __forceinline__ void fft_to_regs_m(typename V2<T>::t *s, int t,
-                                              const typename V2<T>::t *__restrict__ tw,
-                                              Cx<T> out[kVpt], uint32_t rows8) {
+__device__ __forceinline__ void fft_tail_to_regs(typename V2<T>::t *s, int t,
+                                                 const typename V2<T>::t *__restrict__ tw,
+                                                 Cx<T> out[kVpt]) {
   constexpr int N = 1 << LOGN;
   constexpr int P8 = LOGN / 3, REM = LOGN % 3;
   constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
   constexpr int NPASS = P8 + (REM ? 1 : 0);
   static_assert(NPASS >= 2, "the first pass is a radix-8 pass before the last one");
-  stockham_first_pass_m<T, N>(s, t, rows8);
   int Ns = 8;
 #pragma unroll
   for (int p = 1; p < NPASS - 1; p++) {
@@ -291,30 +289,24 @@ __device__ __forceinline__ void fft_to_regs_m(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
-// fft_to_regs with the first pass fed from registers: v[r] is thread t's input
-// at t + r*N/8 (the inputs of its first-pass butterfly), so nothing is stored
-// to shared memory before that butterfly.  The buffer must be free (no thread
-// still reading it) when this is called.
+// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input
+// at t + r*N/8 (its first butterfly's inputs); its outputs go to t*8 + r.  The
+// buffer must be free (no thread still reading it) when this is called.
+template <typename T>
+__device__ __forceinline__ void first_pass_from_regs(typename V2<T>::t *s, int t, Cx<T> v[8]) {
+  Dft<T, 8>::run(v);
+#pragma unroll
+  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
+  __syncthreads();
+}
+
+// fft_to_regs with the first pass fed from registers (as first_pass_from_regs).
 template <typename T, int LOGN>
 __device__ __forceinline__ void fft_to_regs_r(typename V2<T>::t *s, int t,
                                               const typename V2<T>::t *__restrict__ tw,
                                               Cx<T> v[8], Cx<T> out[kVpt]) {
-  constexpr int N = 1 << LOGN;
-  constexpr int P8 = LOGN / 3, REM = LOGN % 3;
-  constexpr int LASTR = REM == 0 ? 8 : (1 << REM);
-  constexpr int NPASS = P8 + (REM ? 1 : 0);
-  static_assert(NPASS >= 2, "the first pass is a radix-8 pass before the last one");
-  Dft<T, 8>::run(v);
-#pragma unroll
-  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
-  __syncthreads();
-  int Ns = 8;
-#pragma unroll
-  for (int p = 1; p < NPASS - 1; p++) {
-    stockham_pass<T, N, 8>(s, t, Ns, tw);
-    Ns *= 8;
-  }
-  stockham_last_pass<T, N, LASTR>(s, t, tw, out);
+  first_pass_from_regs<T>(s, t, v);
+  fft_tail_to_regs<T, LOGN>(s, t, tw, out);
 }
 
 // PP transforms at once, one per shared buffer, sharing every barrier (twice
@@ -451,7 +443,7 @@ __device__ __forceinline__ void fft_row_unit(typename V2<T>::t *s, bool active, 
                                              int nty, int tmw,
                                              const uint32_t *__restrict__ tilemask,
                                              const typename V2<T>::t *__restrict__ tw) {
-  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = padded<T>(N);
   using V = typename V2<T>::t;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
   V *srow = s + grp * LEN;
@@ -570,7 +562,7 @@ template <typename T> struct ColJob {
 // and the row masks of 2*PP planes.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __host__ __device__ constexpr size_t cols_smem_bytes(int rpc) {
-  return (size_t)rpc * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(typename V2<T>::t) *
+  return (size_t)rpc * padded<T>(1 << LOGN) * sizeof(typename V2<T>::t) *
              (DB ? 2 : 1) * PP +
          (RECUR ? (size_t)rpc * (1 << LOGN) * sizeof(typename V2<T>::t) : 0) +
          2 * PP * (size_t)((1 << LOGN) / 32) * 4;
@@ -586,7 +578,7 @@ __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, 
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base,
                                              const ColJob<T> &J) {
-  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = padded<T>(N);
   constexpr int NB = (DB ? 2 : 1) * PP;  // column buffers per row group
   using V = typename V2<T>::t;
   const int rpc = blockDim.x / G;
@@ -639,13 +631,13 @@ __device__ __forceinline__ void fft_col_unit(typename V2<T>::t *s, uint32_t base
         const int k = t + q * G;
         const bool touched = active && ((mask[k >> 5] >> (k & 31)) & 1u);
         if (DB) {
-          cp_async_zfill<T>(dst + pad(k), touched ? col + (uint64_t)k * CB : col, touched);
+          cp_async_zfill<T>(dst + pad<T>(k), touched ? col + (uint64_t)k * CB : col, touched);
         } else {
           V v;
           v.x = 0;
           v.y = 0;
           if (touched) v = col[(uint64_t)k * CB];
-          dst[pad(k)] = v;
+          dst[pad<T>(k)] = v;
         }
       }
     }
@@ -894,33 +886,37 @@ __host__ __device__ constexpr uint32_t tm_cols(int threads) {
   return (uint32_t)(threads / 32 / 4) * 64u;
 }
 
-// Shared memory of the TMEM column pass: NB column buffers per row group and
-// 16 bytes for the TMEM address.
-template <typename T, int LOGN, int NB>
+// Shared memory of the TMEM column pass: a column buffer per row group and 16
+// bytes for the TMEM address.
+template <typename T, int LOGN>
 __host__ __device__ constexpr size_t cols_tm_smem_bytes(int rpc) {
-  return (size_t)rpc * NB * ((1 << LOGN) + (1 << LOGN) / 16) * sizeof(typename V2<T>::t) + 16;
+  return (size_t)rpc * padded<T>(1 << LOGN) * sizeof(typename V2<T>::t) + 16;
 }
 
 // Columns base..base+rpc-1 of one job (one per row group).  The FFT runs in
 // T (FP64 for the plain form, FP32 for the mixed one); the recurrence, its
 // steps and the anchor factor are FP64 in both, so the mixed form adds no
-// phase error to its FP32 transform's.  NB = 2 double-buffers the column
-// loads (the next plane's copies fly during this plane's transform), NB = 1
-// issues them once the transform has read the buffer (each thread's first
-// FFT pass reads exactly the rows it copied, so that pass needs no barrier
-// after the copies).  `taddr` is the thread's TMEM address: its lane quarter
-// and its warp's 64 columns, 8 per pixel q at 8q -- the running sum (re lo/hi,
-// im lo/hi) then the step -- so one 8-column load brings both.
-template <typename T, int LOGN, int NB>
+// phase error to its FP32 transform's.  Only the touched rows of a plane are
+// copied in: thread t copies rows t + q*G (q = 0..7), exactly the inputs of
+// its first-pass butterfly, and reads zero for the untouched ones (bit q of
+// its row mask clear).  The next plane is copied once the transform has read
+// the buffer, during the recurrence; the SM's other blocks cover the rest of
+// the copies' latency.  (A half buffer for the lower rows, copied as soon as
+// the first pass had read them, and a second full buffer where it fits, were
+// both measured slower: 3.86 and 3.14 ms against 3.73 and 3.02 ms for the FP64
+// and FP32 passes at 4096^2 x 32.)  `taddr` is the thread's TMEM address: its
+// lane quarter and its warp's 64 columns, 8 per pixel q at 8q -- the running
+// sum (re lo/hi, im lo/hi) then the step -- so one 8-column load brings both.
+template <typename T, int LOGN>
 __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t base,
                                                 const ColJob<T> &J, uint32_t taddr) {
-  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = N + N / 16;
+  constexpr int N = 1 << LOGN, G = N / kVpt, LEN = padded<T>(N);
   constexpr int CB = col_block<T>();
   using V = typename V2<T>::t;
   const int grp = threadIdx.x / G, t = threadIdx.x % G;
   const int nx = J.nx, ny = J.ny, nw = J.nw, nty = J.nty;
   const uint32_t *__restrict__ counts = J.counts;
-  V *bufs = s + grp * NB * LEN;
+  V *buf = s + grp * LEN;
   const uint32_t n = base + grp;
   const bool active = n < (uint32_t)nx;
   const bool phase = J.phase_on && J.nw_total > 1;
@@ -929,33 +925,31 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
     return iw;
   };
-  // the touched rows of plane iw into buffer b; the untouched ones are left
-  // alone (bit q of the returned mask clear: the first pass reads zero there)
-  auto load_plane = [&](int iw, int b) {
+  // the touched rows t + q*G of plane iw; bit q of the result says whether
+  // row q was copied
+  auto load_rows = [&](int iw) {
     const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
     const V *col = J.cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);
-    V *buf = bufs + b * LEN;
-    uint32_t rows8 = 0;
+    uint32_t bits = 0;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int k = t + q * G;
       const bool touched = active && ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u);
-      if (touched) cp_async_zfill<T>(buf + pad(k), col + (uint64_t)k * CB, true);
-      rows8 |= (touched ? 1u : 0u) << q;
+      if (touched) cp_async_zfill<T>(buf + pad<T>(k), col + (uint64_t)k * CB, true);
+      bits |= (touched ? 1u : 0u) << q;
     }
     cp_async_commit();
-    return rows8;
+    return bits;
   };
-  // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits
-  const double l = active ? J.ltab[n] : 0.0;
+  // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits (l
+  // is read where it is needed rather than held across the transforms)
   auto root_of = [&](int m) {
+    const double l = active ? J.ltab[n] : 0.0;
     const double mm = J.mtab[m];
     return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
   };
   int iw = prev_plane(nw);
-  int cur = 0;  // buffer of plane iw
-  uint32_t rows8 = 0, rows8_next = 0;  // rows of plane iw (of the next plane) copied
-  if (iw >= 0) rows8 = load_plane(iw, cur);
+  uint32_t rows8 = iw >= 0 ? load_rows(iw) : 0u;
   // the per-pixel steps into TMEM
   const double dwstep = __dmul_rn(twopi, J.dw);
 #pragma unroll
@@ -972,17 +966,19 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
   bool first = true;
   int prev = iw;
   while (iw >= 0) {
-    cp_async_wait<0>();
-    if (NB == 2) __syncthreads();  // every copy has landed; the other buffer is free
-    const int nxt = prev_plane(iw);
-    if (NB == 2 && nxt >= 0) rows8_next = load_plane(nxt, cur ^ 1);
+    cp_async_wait<0>();  // this thread's rows of plane iw have landed
+    // first pass: the thread's own rows (zero where not copied)
+    Cx<T> v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+      v[r] = ((rows8 >> r) & 1u) ? lds<T>(buf, t + r * G) : Cx<T>{(T)0, (T)0};
+    __syncthreads();  // every row is read: the buffer is writable
+    first_pass_from_regs<T>(buf, t, v);
     Cx<T> x[kVpt];
-    fft_to_regs_m<T, LOGN>(bufs + cur * LEN, t, J.tw, x, rows8);
-    if (NB == 1) {
-      __syncthreads();  // every thread has read the buffer
-      if (nxt >= 0) rows8_next = load_plane(nxt, cur);
-    }
-    rows8 = rows8_next;
+    fft_tail_to_regs<T, LOGN>(buf, t, J.tw, x);
+    __syncthreads();  // every thread has read the buffer
+    const int nxt = prev_plane(iw);
+    rows8 = nxt >= 0 ? load_rows(nxt) : 0u;
     const int gap = prev - iw;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
@@ -1014,7 +1010,6 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     first = false;
     prev = iw;
     iw = nxt;
-    if (NB == 2) cur ^= 1;
   }
   // image = norm * P * sum, P the factor of the lowest plane with data
   const double cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + prev), J.dw)));
@@ -1049,7 +1044,7 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
 
 template <int LOGN> constexpr int tm_min_blocks() { return 1024 / block_threads<LOGN>(); }
 
-template <typename T, int LOGN, int NB>
+template <typename T, int LOGN>
 __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
     k_fft_cols_tm(ColJob<T> J) {
   constexpr int G = (1 << LOGN) / kVpt;
@@ -1058,7 +1053,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
   const int rpc = blockDim.x / G;
   // the TMEM address slot sits after the column buffers
   uint32_t *slot =
-      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN, NB>(rpc) - 16);
+      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN>(rpc) - 16);
   constexpr uint32_t ncols = tm_cols(block_threads<LOGN>());
   const int warp = threadIdx.x / 32;
   if (warp == 0) {
@@ -1071,7 +1066,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
   const uint32_t tbase = *slot;
   const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 64u;
   for (uint32_t base = blockIdx.x * rpc; base < (uint32_t)J.nx; base += gridDim.x * rpc) {
-    fft_col_unit_tm<T, LOGN, NB>(s, base, J, taddr);
+    fft_col_unit_tm<T, LOGN>(s, base, J, taddr);
     __syncthreads();  // the column buffers are rewritten for the next columns
   }
   tm::fence_before();
@@ -1085,7 +1080,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
 // The TMEM column pass over the jobs col_jobs[lo..hi-1] of a batch (all of FFT
 // length 2^LOGN along y): the column groups of the k-th listed job are
 // col_units[k] .. col_units[k+1]-1.
-template <typename T, int LOGN, int NB>
+template <typename T, int LOGN>
 __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
     k_fft_cols_tm_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
                         int lo, int hi, const uint32_t *__restrict__ col_units,
@@ -1096,7 +1091,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
   auto *s = reinterpret_cast<V *>(smem_raw);
   const int rpc = blockDim.x / G;
   uint32_t *slot =
-      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN, NB>(rpc) - 16);
+      reinterpret_cast<uint32_t *>(smem_raw + cols_tm_smem_bytes<T, LOGN>(rpc) - 16);
   constexpr uint32_t ncols = tm_cols(block_threads<LOGN>());
   const int warp = threadIdx.x / 32;
   if (warp == 0) {
@@ -1132,7 +1127,7 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
     J.phase_on = B.phase_on;
     J.img_re = B.img_re;
     J.img_im = B.img_im;
-    fft_col_unit_tm<T, LOGN, NB>(s, (u - col_units[k]) * (uint32_t)rpc, J, taddr);
+    fft_col_unit_tm<T, LOGN>(s, (u - col_units[k]) * (uint32_t)rpc, J, taddr);
     __syncthreads();
   }
   tm::fence_before();
@@ -1242,7 +1237,7 @@ __global__ void k_fft_units(const BatchJob *__restrict__ jobs, int njobs,
 template <typename T, int LOGN>
 size_t fft_smem(int rpc) {
   constexpr int N = 1 << LOGN;
-  return (size_t)rpc * (N + N / 16) * sizeof(typename V2<T>::t);
+  return (size_t)rpc * padded<T>(N) * sizeof(typename V2<T>::t);
 }
 
 // Longest transform of the multi-job (batch) kernels: 4096.
@@ -1350,34 +1345,34 @@ int launch_cols_impl(const FftJobs &f, const FftClass &c, cudaStream_t st) {
 
 // Implementation choice of the column pass, for measurements: RICK_COLS_TMEM=0
 // selects the register-resident kernels.
-bool env_on(const char *name) {
-  const char *e = getenv(name);
-  return !(e && e[0] == '0');
-}
 bool cols_tm_enabled() {
-  static const bool on = env_on("RICK_COLS_TMEM");
+  static const bool on = [] {
+    const char *e = getenv("RICK_COLS_TMEM");
+    return !(e && e[0] == '0');
+  }();
   return on;
 }
 
-// One job's column pass with the per-pixel state in TMEM.  The dynamic shared
-// memory is padded so that shared memory, not the TMEM allocation, bounds the
-// blocks per SM at 512 / (columns a block allocates): a further block could
-// not allocate and would wait for one of the others to finish.  Column loads
-// are double-buffered when two buffers per block fit beside the other blocks.
-template <typename T, int LOGN, int NB>
-int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int smem_sm,
-                      int reserved) {
+// The column pass with the per-pixel state in TMEM (one job, or the jobs of a
+// batch class).  The dynamic shared memory is padded so that shared memory,
+// not the TMEM allocation, bounds the blocks per SM at 512 / (columns a block
+// allocates): a further block could not allocate and would wait for one of
+// the others to finish.
+template <typename T, int LOGN>
+int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
   const int rpc = BT / G;
   const int max_blocks = (int)(512u / tm_cols(BT));
-  size_t sm = cols_tm_smem_bytes<T, LOGN, NB>(rpc);
+  int dev = 0, smem_sm = 0, reserved = 0;
+  RICK_CUDA(cudaGetDevice(&dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  size_t sm = cols_tm_smem_bytes<T, LOGN>(rpc);
   const size_t floor_b = (size_t)smem_sm / (size_t)(max_blocks + 1) + 1;
   if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
   sm = (sm + 15) & ~(size_t)15;
-  // the whole shared memory as carveout: with the driver's default choice
-  // (164 KB for 77 KB blocks) the SM held one 4096-point block, not two
-  const void *fn = f.one ? (const void *)k_fft_cols_tm<T, LOGN, NB>
-                         : (const void *)k_fft_cols_tm_multi<T, LOGN, NB>;
+  const void *fn = f.one ? (const void *)k_fft_cols_tm<T, LOGN>
+                         : (const void *)k_fft_cols_tm_multi<T, LOGN>;
   RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   // blocks per SM from the kernel's own needs: registers, shared memory, threads
   cudaFuncAttributes fa{};
@@ -1399,26 +1394,14 @@ int launch_cols_tm_nb(const FftJobs &f, const FftClass &c, cudaStream_t st, int 
                                              (uint64_t)num_sms() * per_sm);
   RICK_LAUNCHED();
   if (f.one) {
-    k_fft_cols_tm<T, LOGN, NB><<<blocks, BT, sm, st>>>(col_job<T>(*f.one, f));
+    k_fft_cols_tm<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(*f.one, f));
   } else {
-    k_fft_cols_tm_multi<T, LOGN, NB><<<blocks, BT, sm, st>>>(f.jobs, f.col_jobs, c.lo, c.hi,
-                                                             f.col_units, f.rowmask, f.counts);
+    k_fft_cols_tm_multi<T, LOGN><<<blocks, BT, sm, st>>>(f.jobs, f.col_jobs, c.lo, c.hi,
+                                                         f.col_units, f.rowmask, f.counts);
   }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
-
-template <typename T, int LOGN>
-int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
-  int dev = 0, smem_sm = 0, reserved = 0;
-  RICK_CUDA(cudaGetDevice(&dev));
-  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-  // single-buffered column loads: where two buffers per block fit (FP32), the
-  // double-buffered form measured slower (3.14 against 3.04 ms at 4096^2 x 32)
-  return launch_cols_tm_nb<T, LOGN, 1>(f, c, st, smem_sm, reserved);
-}
-
 
 template <typename T, int LOGN>
 int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {

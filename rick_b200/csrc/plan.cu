@@ -853,11 +853,7 @@ int rick_plan_export_cube(rick_plan *p, double *dst, int dst_is_host, void *stre
     g_launches++;
     return RICK_OK;
   }
-  if (p->d.precision == RICK_PREC_FP64 && scale == 1.0) {
-    RICK_CUDA(cudaMemcpyAsync(dst, p->cube, n * 8, cudaMemcpyDeviceToHost, st));
-    RICK_CUDA(cudaStreamSynchronize(st));
-    return RICK_OK;
-  }
+  if (p->d.precision == RICK_PREC_FP64 && scale == 1.0) return copy_to_host(dst, p->cube, n * 8, st);
   if (!p->d_stage) {
     RICK_TRY(dev_alloc(p, (void **)&p->d_stage, kStageBytes));
     p->stage_bytes = kStageBytes;
@@ -885,8 +881,10 @@ int rick_plan_import_cube(rick_plan *p, const double *src, int src_is_host, void
   cudaStream_t st = (cudaStream_t)stream;
   const uint64_t n = p->cube_vals;
   if (p->d.precision == RICK_PREC_FP64) {
-    RICK_CUDA(cudaMemcpyAsync(p->cube, src, n * 8,
-                              src_is_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+    if (src_is_host)
+      RICK_TRY(copy_to_device(p->cube, src, n * 8, st));
+    else
+      RICK_CUDA(cudaMemcpyAsync(p->cube, src, n * 8, cudaMemcpyDeviceToDevice, st));
   } else {
     const int sms = num_sms();
     if (!src_is_host) {

@@ -276,6 +276,12 @@ int lanes_per_row(uint64_t per_row);
 
 int num_sms();
 
+// Synchronous copies between host memory (pageable or pinned) and device
+// memory; pageable memory goes through a ring of pinned buffers filled and
+// drained by a pool of host threads while the copy engine runs (hostcopy.cu).
+int copy_to_device(void *dst, const void *src, uint64_t bytes, cudaStream_t st);
+int copy_to_host(void *dst, const void *src, uint64_t bytes, cudaStream_t st);
+
 // Kernels launched by this library (reported by rick_launch_count).
 extern std::atomic<unsigned long long> g_launches;
 #define RICK_LAUNCHED() (::rick::g_launches++)

@@ -341,3 +341,35 @@ def test_dropin_sequence_reuses_one_plan(golden):
     before = R.dropin_counters()
     one_round()
     assert R.dropin_counters() == before
+
+
+def test_dropins_on_large_pageable_buffers():
+    """Buffers above the staging chunk (64 MiB) go through the pinned ring and
+    the host thread pool: a 1024^2 x 8 cube (134 MB) through rick_fft_planes
+    and phase_correction, and rows whose sample arrays are 77 MB through
+    wstack, all on pageable numpy memory, against the oracle."""
+    from rick_b200 import synth
+    nx = ny = 1024
+    nw = 8
+    rng = np.random.default_rng(3)
+    grid = rng.standard_normal(2 * nw * nx * ny)
+    got = R.fft_planes(grid, nw, nx, ny)
+    assert rel_l2(got, O.fft_planes(grid, nw, nx, ny)) < TOL_FP64
+    re, im = np.zeros(nx * ny), np.zeros(nx * ny)
+    R.set_phase_on(True)
+    R.phase_correction(got, re, im, nx, ny, nw, nx, ny, 1.0 / 3000.0, -200.0, 180.0)
+    want_re, want_im = O.phase_correction(got, nx, ny, nw, 1.0 / 3000.0, -200.0, 180.0)
+    assert rel_l2(re, want_re) < TOL_FP64 and rel_l2(im, want_im) < TOL_FP64
+    n, nchan, npol = 300_000, 64, 1
+    uu = 0.25 + 0.5 * rng.random(n)
+    vv = 0.25 + 0.5 * rng.random(n)
+    ww = 0.999 * rng.random(n)
+    wt = np.ones(n * npol, dtype=np.float32)
+    vr = rng.standard_normal(n * nchan * npol).astype(np.float32)
+    vi = rng.standard_normal(n * nchan * npol).astype(np.float32)
+    R.set_kernel("kaiser_bessel")
+    g = np.zeros(2 * nw * nx * ny)
+    R.wstack(nw, n, nchan, npol, uu, vv, ww, vr, vi, wt, 1.0 / nx, 1.0 / nw, 7, nx, ny, g)
+    want, _ = O.wstack("kaiser_bessel", nw, nchan, npol, uu, vv, ww, vr, vi, wt, 1.0 / nx,
+                       1.0 / nw, 7, nx, ny)
+    assert rel_l2(g, want) < TOL_FP64
