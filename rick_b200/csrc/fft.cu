@@ -289,7 +289,7 @@ __device__ __forceinline__ void fft_tail_to_regs(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
-// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input
+// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input
 // at t + r*N/8 (its first butterfly's inputs); its outputs go to t*8 + r.  The
 // buffer must be free (no thread still reading it) when this is called.
 template <typename T>
@@ -899,9 +899,12 @@ __host__ __device__ constexpr size_t cols_tm_smem_bytes(int rpc) {
 // phase error to its FP32 transform's.  Only the touched rows of a plane are
 // copied in: thread t copies rows t + q*G (q = 0..7), exactly the inputs of
 // its first-pass butterfly, and reads zero for the untouched ones (bit q of
-// its row mask clear).  The next plane is copied once the transform has read
-// the buffer, during the recurrence; the SM's other blocks cover the rest of
-// the copies' latency.  (A half buffer for the lower rows, copied as soon as
+// its row mask clear).  The next plane's row bits are read before this plane's
+// transform (3.78 -> 3.60 ms FP64, 3.14 -> 2.85 ms FP32 at 4096^2 x 32 against
+// reading them after it); its rows are copied once the transform has read the
+// buffer, during the recurrence, and the SM's other blocks cover the rest of
+// the copies' latency (copying between the last pass's loads and its
+// arithmetic measured slower at 4096 points: 3.78 against 3.60 ms).  (A half buffer for the lower rows, copied as soon as
 // the first pass had read them, and a second full buffer where it fits, were
 // both measured slower: 3.86 and 3.14 ms against 3.73 and 3.02 ms for the FP64
 // and FP32 passes at 4096^2 x 32.)  `taddr` is the thread's TMEM address: its
@@ -925,21 +928,33 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
     return iw;
   };
-  // the touched rows t + q*G of plane iw; bit q of the result says whether
-  // row q was copied
-  auto load_rows = [&](int iw) {
+  // bit q: whether row t + q*G of plane iw was touched (read before the
+  // transform of the plane before it, so that these loads fly during it)
+  auto row_bits = [&](int iw) {
     const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
-    const V *col = J.cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);
     uint32_t bits = 0;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
       const int k = t + q * G;
       const bool touched = active && ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u);
-      if (touched) cp_async_zfill<T>(buf + pad<T>(k), col + (uint64_t)k * CB, true);
       bits |= (touched ? 1u : 0u) << q;
     }
-    cp_async_commit();
     return bits;
+  };
+  // the touched rows t + q*G of plane iw into the buffer
+  auto copy_rows = [&](int iw, uint32_t bits) {
+    const V *col = J.cube + blocked_index<T>(iw, 0, active ? n : 0, nx, ny);
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      const int k = t + q * G;
+      if ((bits >> q) & 1u) cp_async_zfill<T>(buf + pad<T>(k), col + (uint64_t)k * CB, true);
+    }
+    cp_async_commit();
+  };
+  auto load_rows = [&](int iw) {
+    const uint32_t b = row_bits(iw);
+    copy_rows(iw, b);
+    return b;
   };
   // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64, always the same bits (l
   // is read where it is needed rather than held across the transforms)
@@ -967,6 +982,8 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
   int prev = iw;
   while (iw >= 0) {
     cp_async_wait<0>();  // this thread's rows of plane iw have landed
+    const int nxt = prev_plane(iw);
+    const uint32_t next8 = nxt >= 0 ? row_bits(nxt) : 0u;
     // first pass: the thread's own rows (zero where not copied)
     Cx<T> v[8];
 #pragma unroll
@@ -977,8 +994,8 @@ __device__ __forceinline__ void fft_col_unit_tm(typename V2<T>::t *s, uint32_t b
     Cx<T> x[kVpt];
     fft_tail_to_regs<T, LOGN>(buf, t, J.tw, x);
     __syncthreads();  // every thread has read the buffer
-    const int nxt = prev_plane(iw);
-    rows8 = nxt >= 0 ? load_rows(nxt) : 0u;
+    if (nxt >= 0) copy_rows(nxt, next8);
+    rows8 = next8;
     const int gap = prev - iw;
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
