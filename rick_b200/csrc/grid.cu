@@ -46,18 +46,29 @@ struct FixTile {
 };
 template <typename OutT> __host__ __device__ constexpr int fix_bits() { return sizeof(OutT) == 8 ? 61 : 30; }
 
+// The arithmetic type of a footprint cell's contribution: FP64 for the plain
+// form; FP32 for the mixed form, whose tiles are FP32 -- its weights, products
+// and float-to-integer conversions then run on the FP32 pipes (the FP64
+// conversion to integer is a slow instruction), rounding each contribution at
+// about 6e-8 of itself against the 2^-30 of the item's bound the 32-bit sums
+// resolve.
+template <typename OutT> struct Contrib { using type = double; };
+template <> struct Contrib<float> { using type = float; };
+
+__device__ __forceinline__ void fix_put_v(uint32_t *lo, uint32_t *hi, double v) {
+  const long long x = __double2ll_rn(v);
+  const uint32_t l = (uint32_t)(unsigned long long)x;
+  const uint32_t h = (uint32_t)((unsigned long long)x >> 32);
+  const uint32_t old = atomicAdd(lo, l);
+  atomicAdd(hi, h + ((old + l) < old ? 1u : 0u));
+}
+__device__ __forceinline__ void fix_put_v(uint32_t *lo, uint32_t *, float v) {
+  atomicAdd(lo, (uint32_t)__float2int_rn(v));
+}
 template <typename OutT>
-__device__ __forceinline__ void fix_put(uint32_t *lo, uint32_t *hi, double v) {
-  if constexpr (sizeof(OutT) == 8) {
-    const long long x = __double2ll_rn(v);
-    const uint32_t l = (uint32_t)(unsigned long long)x;
-    const uint32_t h = (uint32_t)((unsigned long long)x >> 32);
-    const uint32_t old = atomicAdd(lo, l);
-    atomicAdd(hi, h + ((old + l) < old ? 1u : 0u));
-  } else {
-    (void)hi;
-    atomicAdd(lo, (uint32_t)__double2int_rn(v));
-  }
+__device__ __forceinline__ void fix_put(uint32_t *lo, uint32_t *hi,
+                                        typename Contrib<OutT>::type v) {
+  fix_put_v(lo, hi, v);
 }
 
 template <typename OutT>
@@ -173,18 +184,20 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
         atomicOr(s_rows, bits);
       }
     }
-    const double su = hi ? gnorm * wu : wu;
+    using W = typename Contrib<OutT>::type;
+    const W su = (W)(hi ? gnorm * wu : wu);
+    const W wvw = (W)wv;
     // the scale is a power of two: (s * cw) * scale == (s * scale) * cw exactly
-    const double sre_s = q.sre * scale, sim_s = q.sim * scale;
+    const W sre_s = (W)(q.sre * scale), sim_s = (W)(q.sim * scale);
     // footprint rows e with 0 <= k < ny and y0 <= k < y0 + kTile, k = kb + e
     const int kb = qgv - g.half;
     const int e_lo = max(max(-kb, y0 - kb), 0);
     const int e_hi = min(min(g.ny - kb, y0 + kTile - kb), g.support);
     const int cell0 = (kb - y0) * kPitch + (j - x0);
     for (int e = 0; e < g.support; e++) {
-      const double wve = __shfl_sync(kFull, wv, grp_base + e);
+      const W wve = __shfl_sync(kFull, wvw, grp_base + e);
       if (col_ok && e >= e_lo && e < e_hi) {
-        const double cw = su * wve;
+        const W cw = su * wve;
         const int cell = cell0 + e * kPitch;
         fix_put<OutT>(&tile->lo_re[cell], &tile->hi_re[cell], sre_s * cw);
         fix_put<OutT>(&tile->lo_im[cell], &tile->hi_im[cell], sim_s * cw);
