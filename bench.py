@@ -613,9 +613,22 @@ def run_served(args, dev, stream, ctx, big):
     torch.cuda.empty_cache()  # the pool reserves the whole budget up front
     with R.Server("mixed", device=dev.index or 0, hbm_budget=budget, max_batch_jobs=64,
                   streams=3) as srv:
-        warm = [request(False) for _ in range(8)] + [request(True)]
+        # warm-up: every grid size of the mix at least once (each size's kernels
+        # are loaded on first use), then a few random jobs and a large one
+        sizes = sorted({sp.grid for sp in specs})
+        warm = []
+        for g in sizes:
+            i = next(k for k, sp in enumerate(specs) if sp.grid == g)
+            sp, base = specs[i], ctx["jobs"][i]
+            img = torch.empty(2 * g * g, dtype=torch.float64, device=dev)
+            warm.append((R.Job(R.Geometry(g, g, sp.w_planes, sp.w_support, sp.kernel, "mixed"),
+                               base.nrows, base.freq_per_chan, base.polarizations, base.rows,
+                               base.resolution, base.wmin, base.wmax, img[: g * g], img[g * g:]),
+                         0, 0, img))
+        warm += [request(False) for _ in range(8)] + [request(True)]
         for t in [srv.submit(j) for j, _, _, _ in warm]:
             srv.wait(t)
+        del warm
         for rate in args.served_rates:
             reqs = [request(rng.random() < 0.05) for _ in range(n_req)]
             # rate 0: every request at once (the server's capacity)
