@@ -334,7 +334,11 @@ int build_tables(rick_batch *b, cudaStream_t st) {
   bl.total_row_units = L.total_row_units;
   bl.total_bins = L.total_bins;
   bl.max_support = 1;
-  for (const rick_job_desc &d : b->jobs) bl.max_support = std::max(bl.max_support, d.w_support);
+  bl.min_support = 1 << 30;
+  for (const rick_job_desc &d : b->jobs) {
+    bl.max_support = std::max(bl.max_support, d.w_support);
+    bl.min_support = std::min(bl.min_support, d.w_support);
+  }
   bl.rowmask = (uint32_t *)(A + L.rowmask);
   bl.tilemask = (uint32_t *)(A + L.tilemask);
 

@@ -871,6 +871,34 @@ __device__ __forceinline__ void wait_st4(uint32_t (&r)[4]) {
                : "memory");
 }
 
+// 16 consecutive columns (two pixels' sums and steps); ready after wait_ld16.
+__device__ __forceinline__ void ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void wait_ld16(uint32_t (&a)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]),
+                 "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15])
+               :
+               : "memory");
+}
+// Two 4-column stores in flight: both register sets stay untouched until done.
+__device__ __forceinline__ void wait_st4x2(uint32_t (&a)[4], uint32_t (&b)[4]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(b[0]), "+r"(b[1]),
+                 "+r"(b[2]), "+r"(b[3])
+               :
+               : "memory");
+}
+
 __device__ __forceinline__ double join(uint32_t lo, uint32_t hi) {
   return __hiloint2double((int)hi, (int)lo);
 }
@@ -1155,6 +1183,330 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
   }
 }
 
+// ---- The column pass, two columns per block ---------------------------------
+//
+// A block that transforms one column alternates between the shared-memory pipe
+// (a pass's loads and stores) and the FP64 pipe (its butterflies), and the
+// barriers between the passes keep its warps in step, so the two pipes mostly
+// take turns.  Here one block of N/8 threads holds two columns, A and B, one
+// pass apart: in each barrier interval it computes one pass of one column on
+// values already in registers while it loads the inputs of the other column's
+// next pass, so both pipes are busy at once.  Per plane (N = 4096: a first
+// pass, two middle passes, a last pass to registers) the intervals are
+//   A: read rows | first pass | read | pass 2 | read | pass 3 | read | last + w-step
+//   B: last + w-step (previous plane) | read rows | first pass | read | ... | read
+// The first pass's inputs (the plane's touched rows) come from the cube
+// straight into registers; the next plane's rows are prefetched into L2 a
+// plane ahead.  Each thread holds 16 pixels' running sums and w-steps in TMEM
+// (8 of each column), so a block allocates all 512 TMEM columns of its SM.
+
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
+// v[r] *= w1^r (r = 1..7), the powers formed from w1 as in pass_twiddles.
+template <typename T>
+__device__ __forceinline__ void twiddle8(Cx<T> (&v)[8], typename V2<T>::t a) {
+  const Cx<T> w1 = {a.x, a.y};
+  const Cx<T> w2 = cmul<T>(w1, w1.re, w1.im);
+  const Cx<T> w3 = cmul<T>(w1, w2.re, w2.im);
+  const Cx<T> w4 = cmul<T>(w2, w2.re, w2.im);
+  v[1] = cmul<T>(v[1], w1.re, w1.im);
+  v[2] = cmul<T>(v[2], w2.re, w2.im);
+  v[3] = cmul<T>(v[3], w3.re, w3.im);
+  v[4] = cmul<T>(v[4], w4.re, w4.im);
+  const Cx<T> w5 = cmul<T>(w1, w4.re, w4.im);
+  v[5] = cmul<T>(v[5], w5.re, w5.im);
+  const Cx<T> w6 = cmul<T>(w2, w4.re, w4.im);
+  v[6] = cmul<T>(v[6], w6.re, w6.im);
+  const Cx<T> w7 = cmul<T>(w3, w4.re, w4.im);
+  v[7] = cmul<T>(v[7], w7.re, w7.im);
+}
+
+// the inputs of a pass after the first: values t + r*G
+template <typename T, int N>
+__device__ __forceinline__ void pair_read(const typename V2<T>::t *s, int t, Cx<T> (&v)[8]) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) v[r] = lds<T>(s, t + r * (N / 8));
+}
+// the first pass (stride 1): outputs to t*8 + r
+template <typename T>
+__device__ __forceinline__ void pair_first(typename V2<T>::t *s, int t, Cx<T> (&v)[8]) {
+  Dft<T, 8>::run(v);
+#pragma unroll
+  for (int r = 0; r < 8; r++) sts<T>(s, t * 8 + r, v[r]);
+}
+// a middle pass of stride Ns (butterfly t, twiddle w1 = a)
+template <typename T>
+__device__ __forceinline__ void pair_mid(typename V2<T>::t *s, int t, int Ns,
+                                         typename V2<T>::t a, Cx<T> (&v)[8]) {
+  twiddle8<T>(v, a);
+  Dft<T, 8>::run(v);
+  const int jm = t & (Ns - 1);
+  const int idx = (t - jm) * 8 + jm;
+#pragma unroll
+  for (int r = 0; r < 8; r++) sts<T>(s, idx + r * Ns, v[r]);
+}
+// the last pass (stride N/8): v[r] becomes the transform's value at t + r*G
+template <typename T>
+__device__ __forceinline__ void pair_last(typename V2<T>::t a, Cx<T> (&v)[8]) {
+  twiddle8<T>(v, a);
+  Dft<T, 8>::run(v);
+}
+
+// One w-plane's transform x into the running sums of one column's 8 pixels
+// (TMEM at tcol: pixel q at tcol + 8q, sum then step): sum = sum*step^gap + x,
+// or sum = x for the first plane.
+template <typename T>
+__device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], bool first,
+                                            int gap) {
+#pragma unroll
+  for (int q = 0; q < kVpt; q += 2) {
+    uint32_t a4[2][4];
+    if (first) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        tm::split((double)x[q + h].re, a4[h][0], a4[h][1]);
+        tm::split((double)x[q + h].im, a4[h][2], a4[h][3]);
+      }
+    } else {
+      uint32_t r16[16];
+      tm::ld16(tcol + 8 * q, r16);
+      tm::wait_ld16(r16);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        double ar = tm::join(r16[8 * h + 0], r16[8 * h + 1]);
+        double ai = tm::join(r16[8 * h + 2], r16[8 * h + 3]);
+        const double sr = tm::join(r16[8 * h + 4], r16[8 * h + 5]);
+        const double si = tm::join(r16[8 * h + 6], r16[8 * h + 7]);
+        for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
+          const double tr = fma(ar, sr, -ai * si);
+          ai = fma(ar, si, ai * sr);
+          ar = tr;
+        }
+        const double nr = fma(ar, sr, fma(-ai, si, (double)x[q + h].re));
+        const double ni = fma(ar, si, fma(ai, sr, (double)x[q + h].im));
+        tm::split(nr, a4[h][0], a4[h][1]);
+        tm::split(ni, a4[h][2], a4[h][3]);
+      }
+    }
+    tm::st4(tcol + 8 * q, a4[0]);
+    tm::st4(tcol + 8 * q + 8, a4[1]);
+    tm::wait_st4x2(a4[0], a4[1]);
+  }
+}
+
+// Columns nA and nA + 1 (nA even) of one job; taddr is the thread's TMEM base
+// (column A's pixels at +0, column B's at +64).  The w1 twiddles of the
+// thread's butterflies in passes 2, 3 and the last are read where they are
+// used (L1 hits: 4,096 entries in all).
+template <typename T, int LOGN>
+__device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename V2<T>::t *sB,
+                                                uint32_t nA, const ColJob<T> &J, uint32_t taddr) {
+  static_assert(LOGN == 12, "the pair schedule is written for four radix-8 passes");
+  constexpr int N = 1 << LOGN, G = N / kVpt;
+  constexpr int CB = col_block<T>();
+  using V = typename V2<T>::t;
+  const int t = threadIdx.x;
+  const int nx = J.nx, ny = J.ny, nw = J.nw, nty = J.nty;
+  const uint32_t *__restrict__ counts = J.counts;
+  const bool phase = J.phase_on && J.nw_total > 1;
+  const double twopi = 2.0 * kPi;  // exact doubling of the reference's pi
+  auto prev_plane = [&](int iw) {   // planes without data add exact zeros
+    do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
+    return iw;
+  };
+  // bit q: whether row t + q*G of plane iw was touched (the same for A and B)
+  auto row_bits = [&](int iw) {
+    const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      const int k = t + q * G;
+      bits |= ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u) << q;
+    }
+    return bits;
+  };
+  // the touched rows t + q*G of plane iw of column n (zero elsewhere)
+  auto read_rows = [&](int iw, uint32_t bits, uint32_t n, Cx<T>(&v)[8]) {
+    const V *col = J.cube + blocked_index<T>(iw, 0, n, nx, ny);
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      v[q] = {(T)0, (T)0};
+      if ((bits >> q) & 1u) {
+        const V x = __ldg(col + (uint64_t)(t + q * G) * CB);
+        v[q] = {x.x, x.y};
+      }
+    }
+  };
+  // the same rows into L2 (one 32-byte sector holds both columns' values)
+  auto prefetch_rows = [&](int iw, uint32_t bits) {
+    const V *col = J.cube + blocked_index<T>(iw, 0, nA, nx, ny);
+#pragma unroll
+    for (int q = 0; q < kVpt; q++)
+      if ((bits >> q) & 1u) prefetch_l2(col + (uint64_t)(t + q * G) * CB);
+  };
+  // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64
+  auto root_of = [&](uint32_t n, int m) {
+    const double l = J.ltab[n];
+    const double mm = J.mtab[m];
+    return __dsqrt_rn(__dsub_rn(1.0, __dadd_rn(__dmul_rn(l, l), __dmul_rn(mm, mm))));
+  };
+  int iw = prev_plane(nw);
+  uint32_t bits = iw >= 0 ? row_bits(iw) : 0u;
+  // the per-pixel steps into TMEM
+  const double dwstep = __dmul_rn(twopi, J.dw);
+  const V *__restrict__ tw1 = J.tw + 7 + (t & 7);
+  const V *__restrict__ tw2 = J.tw + 63 + (t & 63);
+  const V *__restrict__ tw3 = J.tw + (N / 8 - 1) + t;
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      const int m = t + q * G;
+      double sn = 0.0, cs = 1.0;
+      if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(nA + c, m), 1.0)), &sn, &cs);
+      uint32_t w4[4];
+      tm::split(cs, w4[0], w4[1]);
+      tm::split(sn, w4[2], w4[3]);
+      tm::st4(taddr + 64 * c + 8 * q + 4, w4);
+      tm::wait_st4(w4);
+    }
+  }
+  Cx<T> vA[8], vB[8];
+  bool first = true, b_pending = false, b_first = true;
+  int prev = iw, b_gap = 0;
+  while (iw >= 0) {
+    // A: the plane's rows | B: last pass and w-step of the previous plane
+    read_rows(iw, bits, nA, vA);
+    const int nxt = prev_plane(iw);
+    const uint32_t nbits = nxt >= 0 ? row_bits(nxt) : 0u;
+    if (b_pending) {
+      pair_last<T>(__ldg(tw3), vB);
+      pair_horner<T>(taddr + 64, vB, b_first, b_gap);
+    }
+    // A: first pass | B: the plane's rows
+    read_rows(iw, bits, nA + 1, vB);
+    pair_first<T>(sA, t, vA);
+    if (nxt >= 0) prefetch_rows(nxt, nbits);
+    __syncthreads();
+    // A: read | B: first pass
+    pair_read<T, N>(sA, t, vA);
+    pair_first<T>(sB, t, vB);
+    __syncthreads();
+    // A: pass 2 | B: read
+    pair_read<T, N>(sB, t, vB);
+    pair_mid<T>(sA, t, 8, __ldg(tw1), vA);
+    __syncthreads();
+    // A: read | B: pass 2
+    pair_read<T, N>(sA, t, vA);
+    pair_mid<T>(sB, t, 8, __ldg(tw1), vB);
+    __syncthreads();
+    // A: pass 3 | B: read
+    pair_read<T, N>(sB, t, vB);
+    pair_mid<T>(sA, t, 64, __ldg(tw2), vA);
+    __syncthreads();
+    // A: read | B: pass 3
+    pair_read<T, N>(sA, t, vA);
+    pair_mid<T>(sB, t, 64, __ldg(tw2), vB);
+    __syncthreads();
+    // A: last pass and w-step | B: read (its last pass runs with the next plane's rows)
+    pair_read<T, N>(sB, t, vB);
+    pair_last<T>(__ldg(tw3), vA);
+    const int gap = prev - iw;
+    pair_horner<T>(taddr, vA, first, gap);
+    b_pending = true;
+    b_first = first;
+    b_gap = gap;
+    first = false;
+    prev = iw;
+    iw = nxt;
+    bits = nbits;
+  }
+  if (b_pending) {
+    pair_last<T>(__ldg(tw3), vB);
+    pair_horner<T>(taddr + 64, vB, b_first, b_gap);
+  }
+  // image = norm * P * sum, P the factor of the lowest plane with data
+  const double cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + prev), J.dw)));
+  const bool vec = ((reinterpret_cast<uintptr_t>(J.img_re) | reinterpret_cast<uintptr_t>(J.img_im)) &
+                    15u) == 0;
+#pragma unroll
+  for (int q = 0; q < kVpt; q++) {
+    const int m = t + q * G;
+    double re[2] = {0.0, 0.0}, im[2] = {0.0, 0.0};
+    if (!first) {
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        uint32_t a4[4];
+        tm::ld4(taddr + 64 * c + 8 * q, a4);
+        tm::wait_ld4(a4);
+        const double ar = tm::join(a4[0], a4[1]);
+        const double ai = tm::join(a4[2], a4[3]);
+        double pr = 1.0, pi = 0.0;
+        if (phase) {
+          const double root = root_of(nA + c, m);
+          double sn, cs;
+          sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
+          const double amp = J.dwnorm * root;
+          pr = cs * amp;
+          pi = sn * amp;
+        }
+        re[c] = J.norm * fma(ar, pr, -ai * pi);
+        im[c] = J.norm * fma(ar, pi, ai * pr);
+      }
+    }
+    const uint64_t o = (uint64_t)m * nx + nA;
+    if (vec) {
+      *reinterpret_cast<double2 *>(J.img_re + o) = make_double2(re[0], re[1]);
+      *reinterpret_cast<double2 *>(J.img_im + o) = make_double2(im[0], im[1]);
+    } else {
+      J.img_re[o] = re[0];
+      J.img_re[o + 1] = re[1];
+      J.img_im[o] = im[0];
+      J.img_im[o + 1] = im[1];
+    }
+  }
+}
+
+template <typename T, int LOGN>
+__host__ __device__ constexpr size_t cols_pair_smem_bytes() {
+  return 2 * (size_t)(1 << LOGN) * sizeof(typename V2<T>::t) + 16;
+}
+
+// One job's column pass, column pairs (nx / 2 of them) over a persistent grid
+// of one block per SM.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(group_threads<LOGN>(), 1) k_fft_cols_pair(ColJob<T> J) {
+  constexpr int N = 1 << LOGN;
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *sA = reinterpret_cast<V *>(smem_raw);
+  V *sB = sA + N;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(smem_raw + cols_pair_smem_bytes<T, LOGN>() - 16);
+  const int warp = threadIdx.x / 32;
+  if (warp == 0) {
+    tm::alloc(slot, 512u);
+    tm::relinquish();
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 128u;
+  const uint32_t pairs = (uint32_t)J.nx / 2u;
+  for (uint32_t p = blockIdx.x; p < pairs; p += gridDim.x) {
+    fft_col_pair_tm<T, LOGN>(sA, sB, 2u * p, J, taddr);
+    __syncthreads();  // the column buffers are rewritten for the next pair
+  }
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    tm::dealloc(tbase, 512u);
+  }
+}
+
 // One job's column pass (the plan): the job as a kernel parameter.
 template <typename T, int LOGN, bool DB, bool RECUR, int PP>
 __global__ void __launch_bounds__(block_threads<LOGN>(), col_min_blocks<T, LOGN, PP>())
@@ -1420,6 +1772,42 @@ int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
+// Implementation choice of the 4096-point column pass, for measurements:
+// RICK_COLS_PAIR=0 selects the one-column TMEM kernel.
+bool cols_pair_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("RICK_COLS_PAIR");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// The two-column pass (one job): one block per SM, which allocates all of the
+// SM's TMEM; its dynamic shared memory is padded above half the SM's so that
+// no second block is placed beside it.
+template <typename T, int LOGN>
+int launch_cols_pair(const BatchJob &B, const FftJobs &f, cudaStream_t st) {
+  constexpr int BT = group_threads<LOGN>();
+  int dev = 0, smem_sm = 0, reserved = 0;
+  RICK_CUDA(cudaGetDevice(&dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  size_t sm = cols_pair_smem_bytes<T, LOGN>();
+  const size_t floor_b = (size_t)smem_sm / 2 + 1;
+  if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
+  sm = (sm + 15) & ~(size_t)15;
+  const void *fn = (const void *)k_fft_cols_pair<T, LOGN>;
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int pct = (int)std::min<size_t>(
+      100, ((sm + (size_t)reserved) * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  const int blocks = std::max(1, std::min(B.g.nx / 2, num_sms()));
+  RICK_LAUNCHED();
+  k_fft_cols_pair<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(B, f));
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
 template <typename T, int LOGN>
 int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
@@ -1429,6 +1817,9 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr size_t kMax = 220 * 1024;
   // the TMEM-state pass: always for one job; for a batch when its schedule
   // asks for it (planes in flight 0) and the length is a batch length
+  if constexpr (LOGN == 12) {
+    if (cols_tm_enabled() && cols_pair_enabled() && f.one) return launch_cols_pair<T, LOGN>(*f.one, f, st);
+  }
   if (cols_tm_enabled() && f.one) return launch_cols_tm<T, LOGN>(f, c, st);
   if constexpr (LOGN <= kMultiMaxLog) {
     if (cols_tm_enabled() && !f.one && f.cols_pp == 0) return launch_cols_tm<T, LOGN>(f, c, st);

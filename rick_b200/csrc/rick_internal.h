@@ -246,6 +246,7 @@ struct BatchLaunch {
   uint64_t total_row_units;
   uint32_t total_bins;
   int max_support;
+  int min_support;
   uint32_t *rowmask, *tilemask;  // batch-wide arrays
   int grid_blocks_per_sm;  // gridder occupancy (tuned)
 };
