@@ -72,7 +72,8 @@ def plan_kernel_name(stage, nx, ny):
     return {"bin_count": "k_bin_count", "bin_scatter": "k_bin_scatter<32,1>",
             "cube_zero": "k_zero_split_tiles<double>", "grid": "k_grid_tiles<double,8>",
             "fft": f"k_fft_rows<double,{lx}>",
-            "phase": f"k_fft_cols_tm<double,{ly}>"}.get(stage, stage)
+            "phase": (f"k_fft_cols_pair<double,{ly}>" if 10 <= ly <= 12
+                      else f"k_fft_cols_tm<double,{ly}>")}.get(stage, stage)
 
 
 def fp64_gemm_tflops(dev) -> float:

@@ -1247,11 +1247,31 @@ __device__ __forceinline__ void pair_mid(typename V2<T>::t *s, int t, int Ns,
 #pragma unroll
   for (int r = 0; r < 8; r++) sts<T>(s, idx + r * Ns, v[r]);
 }
-// the last pass (stride N/8): v[r] becomes the transform's value at t + r*G
-template <typename T>
-__device__ __forceinline__ void pair_last(typename V2<T>::t a, Cx<T> (&v)[8]) {
-  twiddle8<T>(v, a);
-  Dft<T, 8>::run(v);
+// The last pass, of radix R and stride N/R: the thread's B = 8/R butterflies
+// j = t + b*G take v[b + B*r] (the values t + (b + B*r)*G that pair_read
+// brought in) and leave there the transform's value at t + (b + B*r)*G.
+// twl = the thread's first twiddle entry, tw + (N/R - 1) + t.
+template <typename T, int R>
+__device__ __forceinline__ void pair_last(const typename V2<T>::t *__restrict__ twl, int G,
+                                          Cx<T> (&v)[8]) {
+  if constexpr (R == 8) {
+    twiddle8<T>(v, __ldg(twl));
+    Dft<T, 8>::run(v);
+  } else {
+    constexpr int B = 8 / R;
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      Cx<T> u[R], w[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) u[r] = v[b + B * r];
+      pass_twiddles<T, R>(twl + b * G, w);
+#pragma unroll
+      for (int r = 1; r < R; r++) u[r] = cmul<T>(u[r], w[r].re, w[r].im);
+      Dft<T, R>::run(u);
+#pragma unroll
+      for (int r = 0; r < R; r++) v[b + B * r] = u[r];
+    }
+  }
 }
 
 // One w-plane's transform x into the running sums of one column's 8 pixels
@@ -1298,13 +1318,14 @@ __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], 
 
 // Columns nA and nA + 1 (nA even) of one job; taddr is the thread's TMEM base
 // (column A's pixels at +0, column B's at +64).  The w1 twiddles of the
-// thread's butterflies in passes 2, 3 and the last are read where they are
-// used (L1 hits: 4,096 entries in all).
+// thread's butterflies are read where they are used (L1 hits).  For N =
+// 2^LOGN, LOGN = 10..12: a radix-8 first pass, two radix-8 middle passes
+// (strides 8 and 64), a last pass of radix N/512 (stride 512).
 template <typename T, int LOGN>
 __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename V2<T>::t *sB,
                                                 uint32_t nA, const ColJob<T> &J, uint32_t taddr) {
-  static_assert(LOGN == 12, "the pair schedule is written for four radix-8 passes");
-  constexpr int N = 1 << LOGN, G = N / kVpt;
+  static_assert(LOGN >= 10 && LOGN <= 12, "the pair schedule is written for four passes");
+  constexpr int N = 1 << LOGN, G = N / kVpt, LASTR = N / 512;
   constexpr int CB = col_block<T>();
   using V = typename V2<T>::t;
   const int t = threadIdx.x;
@@ -1358,7 +1379,7 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
   const double dwstep = __dmul_rn(twopi, J.dw);
   const V *__restrict__ tw1 = J.tw + 7 + (t & 7);
   const V *__restrict__ tw2 = J.tw + 63 + (t & 63);
-  const V *__restrict__ tw3 = J.tw + (N / 8 - 1) + t;
+  const V *__restrict__ twl = J.tw + (N / LASTR - 1) + t;
 #pragma unroll
   for (int c = 0; c < 2; c++) {
 #pragma unroll
@@ -1382,7 +1403,7 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     const int nxt = prev_plane(iw);
     const uint32_t nbits = nxt >= 0 ? row_bits(nxt) : 0u;
     if (b_pending) {
-      pair_last<T>(__ldg(tw3), vB);
+      pair_last<T, LASTR>(twl, G, vB);
       pair_horner<T>(taddr + 64, vB, b_first, b_gap);
     }
     // A: first pass | B: the plane's rows
@@ -1412,7 +1433,7 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     __syncthreads();
     // A: last pass and w-step | B: read (its last pass runs with the next plane's rows)
     pair_read<T, N>(sB, t, vB);
-    pair_last<T>(__ldg(tw3), vA);
+    pair_last<T, LASTR>(twl, G, vA);
     const int gap = prev - iw;
     pair_horner<T>(taddr, vA, first, gap);
     b_pending = true;
@@ -1424,7 +1445,7 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     bits = nbits;
   }
   if (b_pending) {
-    pair_last<T>(__ldg(tw3), vB);
+    pair_last<T, LASTR>(twl, G, vB);
     pair_horner<T>(taddr + 64, vB, b_first, b_gap);
   }
   // image = norm * P * sum, P the factor of the lowest plane with data
@@ -1474,11 +1495,24 @@ __host__ __device__ constexpr size_t cols_pair_smem_bytes() {
   return 2 * (size_t)(1 << LOGN) * sizeof(typename V2<T>::t) + 16;
 }
 
-// One job's column pass, column pairs (nx / 2 of them) over a persistent grid
-// of one block per SM.
+// TMEM columns a pair block of G threads allocates: 128 per warp of a lane
+// quarter (16 pixels x 8 words).
+__host__ __device__ constexpr uint32_t pair_tm_cols(int threads) {
+  return (uint32_t)(threads / 32 / 4) * 128u;
+}
+
+// One job's column pass, column pairs (nx / 2 of them) over a persistent grid.
+// Blocks of G threads, 512 / G of them per SM (the TMEM they allocate): at most
+// 128 registers a thread.
+template <int LOGN> constexpr int pair_min_blocks() {
+  return (int)(512u / pair_tm_cols(group_threads<LOGN>()));
+}
+
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(group_threads<LOGN>(), 1) k_fft_cols_pair(ColJob<T> J) {
+__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>())
+    k_fft_cols_pair(ColJob<T> J) {
   constexpr int N = 1 << LOGN;
+  constexpr uint32_t ncols = pair_tm_cols(group_threads<LOGN>());
   using V = typename V2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *sA = reinterpret_cast<V *>(smem_raw);
@@ -1486,7 +1520,7 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), 1) k_fft_cols_pair(ColJ
   uint32_t *slot = reinterpret_cast<uint32_t *>(smem_raw + cols_pair_smem_bytes<T, LOGN>() - 16);
   const int warp = threadIdx.x / 32;
   if (warp == 0) {
-    tm::alloc(slot, 512u);
+    tm::alloc(slot, ncols);
     tm::relinquish();
   }
   tm::fence_before();
@@ -1503,7 +1537,68 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), 1) k_fft_cols_pair(ColJ
   __syncthreads();
   if (warp == 0) {
     tm::fence_after();
-    tm::dealloc(tbase, 512u);
+    tm::dealloc(tbase, ncols);
+  }
+}
+
+// The pair pass over the jobs col_jobs[lo..hi-1] of a batch (all of FFT length
+// 2^LOGN along y): the k-th listed job's columns are the global columns
+// col_units[k]*rpc .. col_units[k+1]*rpc - 1 (each job's count even), taken
+// two at a time.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>())
+    k_fft_cols_pair_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
+                          int lo, int hi, const uint32_t *__restrict__ col_units, int rpc,
+                          const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts) {
+  constexpr int N = 1 << LOGN;
+  constexpr uint32_t ncols = pair_tm_cols(group_threads<LOGN>());
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *sA = reinterpret_cast<V *>(smem_raw);
+  V *sB = sA + N;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(smem_raw + cols_pair_smem_bytes<T, LOGN>() - 16);
+  const int warp = threadIdx.x / 32;
+  if (warp == 0) {
+    tm::alloc(slot, ncols);
+    tm::relinquish();
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 128u;
+  const uint32_t p0 = col_units[lo] * (uint32_t)rpc / 2u, p1 = col_units[hi] * (uint32_t)rpc / 2u;
+  for (uint32_t p = p0 + blockIdx.x; p < p1; p += gridDim.x) {
+    const int k = lo + batch_job_of(col_units + lo, hi - lo, 2u * p / (uint32_t)rpc);
+    const BatchJob &B = jobs[col_jobs[k]];
+    ColJob<T> J;
+    J.cube = (const V *)B.blocked;
+    J.nx = B.g.nx;
+    J.ny = B.g.ny;
+    J.nw = B.g.nw;
+    J.nty = B.g.nty;
+    J.w_first = B.g.w_first;
+    J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
+    J.rowmask = rowmask + B.mask_base;
+    J.counts = counts + B.counts_base;
+    J.tw = (const V *)B.tw_y;
+    J.ltab = B.ltab;
+    J.mtab = B.mtab;
+    J.wmin = B.wmin;
+    J.dw = B.dw_phase;
+    J.dwnorm = B.dwnorm;
+    J.norm = B.norm;
+    J.phase_on = B.phase_on;
+    J.img_re = B.img_re;
+    J.img_im = B.img_im;
+    fft_col_pair_tm<T, LOGN>(sA, sB, 2u * p - col_units[k] * (uint32_t)rpc, J, taddr);
+    __syncthreads();
+  }
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    tm::dealloc(tbase, ncols);
   }
 }
 
@@ -1772,8 +1867,8 @@ int launch_cols_tm(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
-// Implementation choice of the 4096-point column pass, for measurements:
-// RICK_COLS_PAIR=0 selects the one-column TMEM kernel.
+// Implementation choice of the 1024- to 4096-point column passes, for
+// measurements: RICK_COLS_PAIR=0 selects the one-column TMEM kernel.
 bool cols_pair_enabled() {
   static const bool on = [] {
     const char *e = getenv("RICK_COLS_PAIR");
@@ -1782,28 +1877,48 @@ bool cols_pair_enabled() {
   return on;
 }
 
-// The two-column pass (one job): one block per SM, which allocates all of the
-// SM's TMEM; its dynamic shared memory is padded above half the SM's so that
-// no second block is placed beside it.
+// The two-column pass (one job, or the jobs of a batch class), for column
+// lengths 1024..4096.  A block of G threads allocates G TMEM columns; its
+// dynamic shared memory is padded so that shared memory, not the TMEM
+// allocation, bounds the blocks per SM (a further block could not allocate).
 template <typename T, int LOGN>
-int launch_cols_pair(const BatchJob &B, const FftJobs &f, cudaStream_t st) {
+int launch_cols_pair(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int BT = group_threads<LOGN>();
+  const int max_blocks = (int)(512u / pair_tm_cols(BT));
   int dev = 0, smem_sm = 0, reserved = 0;
   RICK_CUDA(cudaGetDevice(&dev));
   RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
   RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
   size_t sm = cols_pair_smem_bytes<T, LOGN>();
-  const size_t floor_b = (size_t)smem_sm / 2 + 1;
+  const size_t floor_b = (size_t)smem_sm / (size_t)(max_blocks + 1) + 1;
   if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
   sm = (sm + 15) & ~(size_t)15;
-  const void *fn = (const void *)k_fft_cols_pair<T, LOGN>;
+  const void *fn = f.one ? (const void *)k_fft_cols_pair<T, LOGN>
+                         : (const void *)k_fft_cols_pair_multi<T, LOGN>;
   RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  cudaFuncAttributes fa{};
+  RICK_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const int regs_per_warp = ((std::max(fa.numRegs, 1) * 32 + 255) / 256) * 256;
+  const int by_regs = 65536 / (regs_per_warp * (BT / 32));
+  const int by_smem = (int)((size_t)smem_sm / (sm + (size_t)reserved));
+  const int by_threads = 2048 / BT;
+  const int per_sm = std::max(1, std::min({max_blocks, by_regs, by_smem, by_threads}));
   const int pct = (int)std::min<size_t>(
-      100, ((sm + (size_t)reserved) * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+      100, ((size_t)per_sm * (sm + (size_t)reserved) * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
   RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
-  const int blocks = std::max(1, std::min(B.g.nx / 2, num_sms()));
+  const uint64_t slots = (uint64_t)num_sms() * per_sm;
   RICK_LAUNCHED();
-  k_fft_cols_pair<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(B, f));
+  if (f.one) {
+    const BatchJob &B = *f.one;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)B.g.nx / 2, slots));
+    k_fft_cols_pair<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(B, f));
+  } else {
+    const int rpc = fft_rows_per_block(LOGN);
+    const uint64_t pairs = (uint64_t)c.units * (uint64_t)rpc / 2u;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(pairs, slots));
+    k_fft_cols_pair_multi<T, LOGN><<<blocks, BT, sm, st>>>(f.jobs, f.col_jobs, c.lo, c.hi,
+                                                           f.col_units, rpc, f.rowmask, f.counts);
+  }
   RICK_CUDA(cudaGetLastError());
   return RICK_OK;
 }
@@ -1815,14 +1930,17 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   // in order of preference, the first that fits: two planes per iteration
   // (FP32), double-buffered loads, the per-pixel phase steps
   constexpr size_t kMax = 220 * 1024;
-  // the TMEM-state pass: always for one job; for a batch when its schedule
-  // asks for it (planes in flight 0) and the length is a batch length
-  if constexpr (LOGN == 12) {
-    if (cols_tm_enabled() && cols_pair_enabled() && f.one) return launch_cols_pair<T, LOGN>(*f.one, f, st);
+  // the TMEM-state passes: always for one job; for a batch when its schedule
+  // asks for them (planes in flight 0).  Two columns per block from 1024 to
+  // 4096 points (both columns' buffers in shared memory), one below and above.
+  const bool tm_one = cols_tm_enabled() && f.one;
+  const bool tm_batch = cols_tm_enabled() && !f.one && f.cols_pp == 0 && LOGN <= kMultiMaxLog;
+  if constexpr (LOGN >= 10 && LOGN <= 12) {
+    if ((tm_one || tm_batch) && cols_pair_enabled()) return launch_cols_pair<T, LOGN>(f, c, st);
   }
-  if (cols_tm_enabled() && f.one) return launch_cols_tm<T, LOGN>(f, c, st);
+  if (tm_one) return launch_cols_tm<T, LOGN>(f, c, st);
   if constexpr (LOGN <= kMultiMaxLog) {
-    if (cols_tm_enabled() && !f.one && f.cols_pp == 0) return launch_cols_tm<T, LOGN>(f, c, st);
+    if (tm_batch) return launch_cols_tm<T, LOGN>(f, c, st);
   }
 #define RICK_TRY_COLS(DB, RC, PP)                            \
   if (cols_smem<T, LOGN, DB, RC, PP>(rpc) <= kMax)           \
