@@ -890,6 +890,39 @@ __device__ __forceinline__ void wait_ld16(uint32_t (&a)[16]) {
                :
                : "memory");
 }
+__device__ __forceinline__ void ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void wait_ld32(uint32_t (&a)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]),
+                 "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]), "+r"(a[16]), "+r"(a[17]),
+                 "+r"(a[18]), "+r"(a[19]), "+r"(a[20]), "+r"(a[21]), "+r"(a[22]), "+r"(a[23]),
+                 "+r"(a[24]), "+r"(a[25]), "+r"(a[26]), "+r"(a[27]), "+r"(a[28]), "+r"(a[29]),
+                 "+r"(a[30]), "+r"(a[31])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void wait_st4x4(uint32_t (&a)[4][4]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n"
+               : "+r"(a[0][0]), "+r"(a[0][1]), "+r"(a[0][2]), "+r"(a[0][3]), "+r"(a[1][0]),
+                 "+r"(a[1][1]), "+r"(a[1][2]), "+r"(a[1][3]), "+r"(a[2][0]), "+r"(a[2][1]),
+                 "+r"(a[2][2]), "+r"(a[2][3]), "+r"(a[3][0]), "+r"(a[3][1]), "+r"(a[3][2]),
+                 "+r"(a[3][3])
+               :
+               : "memory");
+}
 // Two 4-column stores in flight: both register sets stay untouched until done.
 __device__ __forceinline__ void wait_st4x2(uint32_t (&a)[4], uint32_t (&b)[4]) {
   asm volatile("tcgen05.wait::st.sync.aligned;\n"
@@ -1276,29 +1309,37 @@ __device__ __forceinline__ void pair_last(const typename V2<T>::t *__restrict__ 
 
 // One w-plane's transform x into the running sums of one column's 8 pixels
 // (TMEM at tcol: pixel q at tcol + 8q, sum then step): sum = sum*step^gap + x,
-// or sum = x for the first plane.
+// or sum = x for the first plane.  PX pixels per TMEM access: 4 for the FP32
+// transform (2.68 -> 2.61 ms for the mixed form's column pass at 4096^2 x 32),
+// 2 for the FP64 one, whose registers hold twice the transform values.
 template <typename T>
 __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], bool first,
                                             int gap) {
+  constexpr int PX = sizeof(T) == 4 ? 4 : 2;
 #pragma unroll
-  for (int q = 0; q < kVpt; q += 2) {
-    uint32_t a4[2][4];
+  for (int q = 0; q < kVpt; q += PX) {
+    uint32_t a4[PX][4];
     if (first) {
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < PX; h++) {
         tm::split((double)x[q + h].re, a4[h][0], a4[h][1]);
         tm::split((double)x[q + h].im, a4[h][2], a4[h][3]);
       }
     } else {
-      uint32_t r16[16];
-      tm::ld16(tcol + 8 * q, r16);
-      tm::wait_ld16(r16);
+      uint32_t r[8 * PX];
+      if constexpr (PX == 4) {
+        tm::ld32(tcol + 8 * q, r);
+        tm::wait_ld32(r);
+      } else {
+        tm::ld16(tcol + 8 * q, r);
+        tm::wait_ld16(r);
+      }
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        double ar = tm::join(r16[8 * h + 0], r16[8 * h + 1]);
-        double ai = tm::join(r16[8 * h + 2], r16[8 * h + 3]);
-        const double sr = tm::join(r16[8 * h + 4], r16[8 * h + 5]);
-        const double si = tm::join(r16[8 * h + 6], r16[8 * h + 7]);
+      for (int h = 0; h < PX; h++) {
+        double ar = tm::join(r[8 * h + 0], r[8 * h + 1]);
+        double ai = tm::join(r[8 * h + 2], r[8 * h + 3]);
+        const double sr = tm::join(r[8 * h + 4], r[8 * h + 5]);
+        const double si = tm::join(r[8 * h + 6], r[8 * h + 7]);
         for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
           const double tr = fma(ar, sr, -ai * si);
           ai = fma(ar, si, ai * sr);
@@ -1310,9 +1351,12 @@ __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], 
         tm::split(ni, a4[h][2], a4[h][3]);
       }
     }
-    tm::st4(tcol + 8 * q, a4[0]);
-    tm::st4(tcol + 8 * q + 8, a4[1]);
-    tm::wait_st4x2(a4[0], a4[1]);
+#pragma unroll
+    for (int h = 0; h < PX; h++) tm::st4(tcol + 8 * (q + h), a4[h]);
+    if constexpr (PX == 4)
+      tm::wait_st4x4(a4);
+    else
+      tm::wait_st4x2(a4[0], a4[1]);
   }
 }
 

@@ -253,8 +253,10 @@ __device__ __forceinline__ uint32_t bin_of_item(const uint32_t *__restrict__ ite
   return lo;
 }
 
+// Six blocks per SM (the launch's grid): registers bounded to 40 a thread
+// (c2 FP64 gridder 1.00 -> 0.955 ms against the compiler's own choice, five).
 template <typename OutT, int LPR, int SUP = 0>
-__global__ void __launch_bounds__(kGridThreads)
+__global__ void __launch_bounds__(kGridThreads, 6)
     k_grid_tiles(const RecF64 *__restrict__ rec, const uint32_t *__restrict__ bin_off,
                  const uint32_t *__restrict__ item_off, uint32_t nbins, uint32_t max_chunk,
                  Geometry g, int kernel, const double *__restrict__ table, int accumulate,
