@@ -57,6 +57,8 @@ WORKLOAD_TEXT = {
 # captures of a kernel on a workload at full size, keyed by (workload, kernel);
 # each entry names the capture.  A kernel without a capture reports null.
 NCU_TRAFFIC = {
+    ("c2", "k_fft_cols_pair<double,12>"): (2_312_723_797, "profiles/traffic_c2.md (mean of 3 "
+                                           "launches, one-pass dram__bytes_read/write capture)"),
     ("c2", "k_fft_cols_tm<double,12>"): (2_383_968_341, "profiles/traffic_c2.md (mean of 3 "
                                          "launches, one-pass dram__bytes_read/write capture)"),
     ("c2", "k_bin_scatter<32,1>"): (10_851_913_216, "profiles/traffic_c2.md"),
