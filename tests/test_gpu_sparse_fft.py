@@ -142,3 +142,59 @@ def test_mixed_phase_recurrence_skips_empty_planes():
                               selection=R.ROWS_ALL, precision=precision)
         err = rel_l2(np.concatenate([re, im]), np.concatenate([want_re, want_im]))
         assert err < tol, (precision, err)
+
+
+def _pair_case_rows(seed, n, nw, planes=None):
+    rng = np.random.default_rng(seed)
+    if planes is None:
+        ww = rng.random(n) * 0.999
+    else:
+        planes = np.asarray(planes)
+        ww = (planes[rng.integers(0, len(planes), n)] + rng.uniform(0.1, 0.9, n)) / nw
+    uu = np.clip(0.5 + 0.2 * rng.standard_normal(n), 0, 1)
+    vv = np.clip(0.5 + 0.2 * rng.standard_normal(n), 0, 0.9999)
+    return (uu, vv, ww, rng.uniform(0.5, 1.5, 2 * n).astype(np.float32),
+            rng.standard_normal(2 * n).astype(np.float32),
+            rng.standard_normal(2 * n).astype(np.float32))
+
+
+@pytest.mark.parametrize("nx,ny,nw,phase_on,planes", [
+    (128, 2048, 5, True, None),                 # 2048-point columns (radix-4 last pass)
+    (64, 1024, 6, False, None),                 # 1024-point columns (radix-2), phase off
+    (256, 1024, 16, True, [1, 2, 5, 13, 14]),   # planes without rows between planes with rows
+    (64, 4096, 7, True, [0, 6]),                # the first and last planes only
+])
+def test_two_column_pass_vs_oracle(nx, ny, nw, phase_on, planes):
+    """Column lengths 1024..4096 run two columns per block, one pass apart:
+    each form against the oracle, including plane gaps and PHASE_ON off."""
+    n = 5000
+    host = _pair_case_rows(nx + ny + nw, n, nw, planes)
+    rows = gpu_rows(*host)
+    res, wmin, wmax = 1.0 / (2.3 * max(nx, ny)), -700.0, 650.0
+    want_re, want_im = _oracle_image(host, nx, ny, nw, "kaiser_bessel", 7, 1, 2, res, wmin, wmax,
+                                     phase_on=phase_on)
+    want = np.concatenate([want_re, want_im])
+    for precision, tol in (("fp64", TOL_FP64), ("mixed", TOL_MIXED)):
+        re, im, _ = gpu_image(rows, n, nx, ny, nw, 7, "kaiser_bessel", 1, 2, res, wmin, wmax,
+                              selection=R.ROWS_ALL, precision=precision, phase_on=phase_on)
+        err = rel_l2(np.concatenate([re, im]), want)
+        assert err < tol, (precision, err)
+
+
+def test_image_rows_at_an_odd_address():
+    """Image arrays that do not start on a 16-byte boundary (one double past
+    it): the column pass writes them element by element, with the same values."""
+    import torch
+    nx, ny, nw, n = 128, 4096, 4, 4000
+    host = _pair_case_rows(5, n, nw)
+    rows = gpu_rows(*host)
+    res, wmin, wmax = 1.0 / 9000.0, -300.0, 280.0
+    want_re, want_im = _oracle_image(host, nx, ny, nw, "kaiser_bessel", 7, 1, 2, res, wmin, wmax)
+    geom = R.Geometry(nx, ny, nw, 7, "kaiser_bessel", "fp64")
+    with R.Plan(geom, n, 1, 2, device=0) as plan:
+        buf = torch.full((2 * nx * ny + 1,), float("nan"), dtype=torch.float64, device="cuda")
+        plan.image(n, rows, res, wmin, wmax, buf[1: 1 + nx * ny], buf[1 + nx * ny:], R.ROWS_ALL)
+        torch.cuda.synchronize()
+        got = buf.cpu().numpy()
+    assert np.isnan(got[0])
+    assert rel_l2(got[1:], np.concatenate([want_re, want_im])) < TOL_FP64
