@@ -289,7 +289,7 @@ __device__ __forceinline__ void fft_tail_to_regs(typename V2<T>::t *s, int t,
   stockham_last_pass<T, N, LASTR>(s, t, tw, out);
 }
 
-// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input
+// The first pass (stride 1, radix 8) from registers: v[r] is thread t's input
 // at t + r*N/8 (its first butterfly's inputs); its outputs go to t*8 + r.  The
 // buffer must be free (no thread still reading it) when this is called.
 template <typename T>
@@ -1224,14 +1224,18 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
 // take turns.  Here one block of N/8 threads holds two columns, A and B, one
 // pass apart: in each barrier interval it computes one pass of one column on
 // values already in registers while it loads the inputs of the other column's
-// next pass, so both pipes are busy at once.  Per plane (N = 4096: a first
-// pass, two middle passes, a last pass to registers) the intervals are
+// next pass, so both pipes are busy at once.  Per plane (N = 1024..4096: a
+// first pass, two middle passes, a last pass of radix N/512 to registers) the
+// intervals are
 //   A: read rows | first pass | read | pass 2 | read | pass 3 | read | last + w-step
 //   B: last + w-step (previous plane) | read rows | first pass | read | ... | read
+// with a barrier after each interval from the second to the seventh (the
+// first two and the last touch no shared memory the other threads use next).
 // The first pass's inputs (the plane's touched rows) come from the cube
 // straight into registers; the next plane's rows are prefetched into L2 a
 // plane ahead.  Each thread holds 16 pixels' running sums and w-steps in TMEM
-// (8 of each column), so a block allocates all 512 TMEM columns of its SM.
+// (8 of each column): a block of N/8 threads allocates N/8 TMEM columns, all
+// 512 of its SM at N = 4096.
 
 __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
