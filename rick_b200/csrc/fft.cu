@@ -890,36 +890,36 @@ __device__ __forceinline__ void wait_ld16(uint32_t (&a)[16]) {
                :
                : "memory");
 }
-__device__ __forceinline__ void ld32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-      "%30, %31}, [%32];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr)
-      : "memory");
-}
-__device__ __forceinline__ void wait_ld32(uint32_t (&a)[32]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
-               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
-                 "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]),
-                 "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]), "+r"(a[16]), "+r"(a[17]),
-                 "+r"(a[18]), "+r"(a[19]), "+r"(a[20]), "+r"(a[21]), "+r"(a[22]), "+r"(a[23]),
-                 "+r"(a[24]), "+r"(a[25]), "+r"(a[26]), "+r"(a[27]), "+r"(a[28]), "+r"(a[29]),
-                 "+r"(a[30]), "+r"(a[31])
-               :
+__device__ __forceinline__ void st2(uint32_t taddr, const uint32_t (&r)[2]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n" ::"r"(taddr), "r"(r[0]),
+               "r"(r[1])
                : "memory");
 }
-__device__ __forceinline__ void wait_st4x4(uint32_t (&a)[4][4]) {
+__device__ __forceinline__ void wait_st2(uint32_t (&r)[2]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n" : "+r"(r[0]), "+r"(r[1]) : : "memory");
+}
+__device__ __forceinline__ void ld2(uint32_t taddr, uint32_t (&r)[2]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n"
+               : "=r"(r[0]), "=r"(r[1])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void wait_ld2(uint32_t (&a)[2]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(a[0]), "+r"(a[1]) : : "memory");
+}
+__device__ __forceinline__ void st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};\n" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void wait_st16(uint32_t (&a)[16]) {
   asm volatile("tcgen05.wait::st.sync.aligned;\n"
-               : "+r"(a[0][0]), "+r"(a[0][1]), "+r"(a[0][2]), "+r"(a[0][3]), "+r"(a[1][0]),
-                 "+r"(a[1][1]), "+r"(a[1][2]), "+r"(a[1][3]), "+r"(a[2][0]), "+r"(a[2][1]),
-                 "+r"(a[2][2]), "+r"(a[2][3]), "+r"(a[3][0]), "+r"(a[3][1]), "+r"(a[3][2]),
-                 "+r"(a[3][3])
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]),
+                 "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15])
                :
                : "memory");
 }
@@ -1311,61 +1311,100 @@ __device__ __forceinline__ void pair_last(const typename V2<T>::t *__restrict__ 
   }
 }
 
+// TMEM words a pixel's running sum and w-step take in the two-column pass: FP64
+// complex pairs (8) for the FP64 transform, FP32 pairs (4) for the FP32 one.
+// The FP32 recurrence adds ~4e-7 relative error over 32 planes (modelled at
+// 4096^2 x 32, w from -7.5e3 to 7.8e3 wavelengths), within the FP32
+// transform's own; with half the TMEM, two 4096-point blocks share an SM.
+template <typename T> __host__ __device__ constexpr uint32_t pair_pixel_words() {
+  return sizeof(T) == 8 ? 8u : 4u;
+}
+
 // One w-plane's transform x into the running sums of one column's 8 pixels
-// (TMEM at tcol: pixel q at tcol + 8q, sum then step): sum = sum*step^gap + x,
-// or sum = x for the first plane.  PX pixels per TMEM access: 4 for the FP32
-// transform (2.68 -> 2.61 ms for the mixed form's column pass at 4096^2 x 32),
-// 2 for the FP64 one, whose registers hold twice the transform values.
+// (TMEM at tcol: pixel q at tcol + W*q, W = pair_pixel_words, sum then step):
+// sum = sum*step^gap + x, or sum = x for the first plane.  FP64 state: two
+// pixels per TMEM access; FP32 state: four.
 template <typename T>
 __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], bool first,
                                             int gap) {
-  constexpr int PX = sizeof(T) == 4 ? 4 : 2;
+  if constexpr (sizeof(T) == 4) {
 #pragma unroll
-  for (int q = 0; q < kVpt; q += PX) {
-    uint32_t a4[PX][4];
-    if (first) {
+    for (int q = 0; q < kVpt; q += 4) {
+      uint32_t r[16];
+      if (first) {
 #pragma unroll
-      for (int h = 0; h < PX; h++) {
-        tm::split((double)x[q + h].re, a4[h][0], a4[h][1]);
-        tm::split((double)x[q + h].im, a4[h][2], a4[h][3]);
-      }
-    } else {
-      uint32_t r[8 * PX];
-      if constexpr (PX == 4) {
-        tm::ld32(tcol + 8 * q, r);
-        tm::wait_ld32(r);
-      } else {
-        tm::ld16(tcol + 8 * q, r);
-        tm::wait_ld16(r);
-      }
-#pragma unroll
-      for (int h = 0; h < PX; h++) {
-        double ar = tm::join(r[8 * h + 0], r[8 * h + 1]);
-        double ai = tm::join(r[8 * h + 2], r[8 * h + 3]);
-        const double sr = tm::join(r[8 * h + 4], r[8 * h + 5]);
-        const double si = tm::join(r[8 * h + 6], r[8 * h + 7]);
-        for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
-          const double tr = fma(ar, sr, -ai * si);
-          ai = fma(ar, si, ai * sr);
-          ar = tr;
+        for (int h = 0; h < 4; h++) {
+          r[4 * h + 0] = __float_as_uint(x[q + h].re);
+          r[4 * h + 1] = __float_as_uint(x[q + h].im);
         }
-        const double nr = fma(ar, sr, fma(-ai, si, (double)x[q + h].re));
-        const double ni = fma(ar, si, fma(ai, sr, (double)x[q + h].im));
-        tm::split(nr, a4[h][0], a4[h][1]);
-        tm::split(ni, a4[h][2], a4[h][3]);
+        // the steps are kept: write the sums only
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          uint32_t a2[2] = {r[4 * h + 0], r[4 * h + 1]};
+          tm::st2(tcol + 4 * (q + h), a2);
+          tm::wait_st2(a2);
+        }
+      } else {
+        tm::ld16(tcol + 4 * q, r);
+        tm::wait_ld16(r);
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          float ar = __uint_as_float(r[4 * h + 0]);
+          float ai = __uint_as_float(r[4 * h + 1]);
+          const float sr = __uint_as_float(r[4 * h + 2]);
+          const float si = __uint_as_float(r[4 * h + 3]);
+          for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
+            const float tr = fmaf(ar, sr, -ai * si);
+            ai = fmaf(ar, si, ai * sr);
+            ar = tr;
+          }
+          r[4 * h + 0] = __float_as_uint(fmaf(ar, sr, fmaf(-ai, si, (float)x[q + h].re)));
+          r[4 * h + 1] = __float_as_uint(fmaf(ar, si, fmaf(ai, sr, (float)x[q + h].im)));
+        }
+        tm::st16(tcol + 4 * q, r);
+        tm::wait_st16(r);
       }
     }
+  } else {
 #pragma unroll
-    for (int h = 0; h < PX; h++) tm::st4(tcol + 8 * (q + h), a4[h]);
-    if constexpr (PX == 4)
-      tm::wait_st4x4(a4);
-    else
+    for (int q = 0; q < kVpt; q += 2) {
+      uint32_t a4[2][4];
+      if (first) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          tm::split((double)x[q + h].re, a4[h][0], a4[h][1]);
+          tm::split((double)x[q + h].im, a4[h][2], a4[h][3]);
+        }
+      } else {
+        uint32_t r[16];
+        tm::ld16(tcol + 8 * q, r);
+        tm::wait_ld16(r);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          double ar = tm::join(r[8 * h + 0], r[8 * h + 1]);
+          double ai = tm::join(r[8 * h + 2], r[8 * h + 3]);
+          const double sr = tm::join(r[8 * h + 4], r[8 * h + 5]);
+          const double si = tm::join(r[8 * h + 6], r[8 * h + 7]);
+          for (int g2 = 1; g2 < gap; g2++) {  // planes without data in between
+            const double tr = fma(ar, sr, -ai * si);
+            ai = fma(ar, si, ai * sr);
+            ar = tr;
+          }
+          const double nr = fma(ar, sr, fma(-ai, si, (double)x[q + h].re));
+          const double ni = fma(ar, si, fma(ai, sr, (double)x[q + h].im));
+          tm::split(nr, a4[h][0], a4[h][1]);
+          tm::split(ni, a4[h][2], a4[h][3]);
+        }
+      }
+      tm::st4(tcol + 8 * q, a4[0]);
+      tm::st4(tcol + 8 * q + 8, a4[1]);
       tm::wait_st4x2(a4[0], a4[1]);
+    }
   }
 }
 
 // Columns nA and nA + 1 (nA even) of one job; taddr is the thread's TMEM base
-// (column A's pixels at +0, column B's at +64).  The w1 twiddles of the
+// (column A's pixels at +0, column B's at +8W, W = pair_pixel_words).  The w1 twiddles of the
 // thread's butterflies are read where they are used (L1 hits).  For N =
 // 2^LOGN, LOGN = 10..12: a radix-8 first pass, two radix-8 middle passes
 // (strides 8 and 64), a last pass of radix N/512 (stride 512).
@@ -1425,9 +1464,11 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
   uint32_t bits = iw >= 0 ? row_bits(iw) : 0u;
   // the per-pixel steps into TMEM
   const double dwstep = __dmul_rn(twopi, J.dw);
-  const V *__restrict__ tw1 = J.tw + 7 + (t & 7);
-  const V *__restrict__ tw2 = J.tw + 63 + (t & 63);
-  const V *__restrict__ twl = J.tw + (N / LASTR - 1) + t;
+  // the thread's twiddle entries, formed where used (fewer live registers)
+  auto tw1 = [&] { return J.tw + 7 + (t & 7); };
+  auto tw2 = [&] { return J.tw + 63 + (t & 63); };
+  auto twl = [&] { return J.tw + (N / LASTR - 1) + t; };
+  constexpr uint32_t PW = pair_pixel_words<T>(), tB = 8 * PW;  // column B's TMEM offset
 #pragma unroll
   for (int c = 0; c < 2; c++) {
 #pragma unroll
@@ -1435,11 +1476,17 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
       const int m = t + q * G;
       double sn = 0.0, cs = 1.0;
       if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(nA + c, m), 1.0)), &sn, &cs);
-      uint32_t w4[4];
-      tm::split(cs, w4[0], w4[1]);
-      tm::split(sn, w4[2], w4[3]);
-      tm::st4(taddr + 64 * c + 8 * q + 4, w4);
-      tm::wait_st4(w4);
+      if constexpr (PW == 8) {
+        uint32_t w4[4];
+        tm::split(cs, w4[0], w4[1]);
+        tm::split(sn, w4[2], w4[3]);
+        tm::st4(taddr + tB * c + PW * q + 4, w4);
+        tm::wait_st4(w4);
+      } else {
+        uint32_t w2[2] = {__float_as_uint((float)cs), __float_as_uint((float)sn)};
+        tm::st2(taddr + tB * c + PW * q + 2, w2);
+        tm::wait_st2(w2);
+      }
     }
   }
   Cx<T> vA[8], vB[8];
@@ -1451,8 +1498,8 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     const int nxt = prev_plane(iw);
     const uint32_t nbits = nxt >= 0 ? row_bits(nxt) : 0u;
     if (b_pending) {
-      pair_last<T, LASTR>(twl, G, vB);
-      pair_horner<T>(taddr + 64, vB, b_first, b_gap);
+      pair_last<T, LASTR>(twl(), G, vB);
+      pair_horner<T>(taddr + tB, vB, b_first, b_gap);
     }
     // A: first pass | B: the plane's rows
     read_rows(iw, bits, nA + 1, vB);
@@ -1465,23 +1512,23 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     __syncthreads();
     // A: pass 2 | B: read
     pair_read<T, N>(sB, t, vB);
-    pair_mid<T>(sA, t, 8, __ldg(tw1), vA);
+    pair_mid<T>(sA, t, 8, __ldg(tw1()), vA);
     __syncthreads();
     // A: read | B: pass 2
     pair_read<T, N>(sA, t, vA);
-    pair_mid<T>(sB, t, 8, __ldg(tw1), vB);
+    pair_mid<T>(sB, t, 8, __ldg(tw1()), vB);
     __syncthreads();
     // A: pass 3 | B: read
     pair_read<T, N>(sB, t, vB);
-    pair_mid<T>(sA, t, 64, __ldg(tw2), vA);
+    pair_mid<T>(sA, t, 64, __ldg(tw2()), vA);
     __syncthreads();
     // A: read | B: pass 3
     pair_read<T, N>(sA, t, vA);
-    pair_mid<T>(sB, t, 64, __ldg(tw2), vB);
+    pair_mid<T>(sB, t, 64, __ldg(tw2()), vB);
     __syncthreads();
     // A: last pass and w-step | B: read (its last pass runs with the next plane's rows)
     pair_read<T, N>(sB, t, vB);
-    pair_last<T, LASTR>(twl, G, vA);
+    pair_last<T, LASTR>(twl(), G, vA);
     const int gap = prev - iw;
     pair_horner<T>(taddr, vA, first, gap);
     b_pending = true;
@@ -1493,8 +1540,8 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     bits = nbits;
   }
   if (b_pending) {
-    pair_last<T, LASTR>(twl, G, vB);
-    pair_horner<T>(taddr + 64, vB, b_first, b_gap);
+    pair_last<T, LASTR>(twl(), G, vB);
+    pair_horner<T>(taddr + tB, vB, b_first, b_gap);
   }
   // image = norm * P * sum, P the factor of the lowest plane with data
   const double cw = __dmul_rn(twopi, __dadd_rn(J.wmin, __dmul_rn((double)(J.w_first + prev), J.dw)));
@@ -1507,11 +1554,20 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     if (!first) {
 #pragma unroll
       for (int c = 0; c < 2; c++) {
-        uint32_t a4[4];
-        tm::ld4(taddr + 64 * c + 8 * q, a4);
-        tm::wait_ld4(a4);
-        const double ar = tm::join(a4[0], a4[1]);
-        const double ai = tm::join(a4[2], a4[3]);
+        double ar, ai;
+        if constexpr (PW == 8) {
+          uint32_t a4[4];
+          tm::ld4(taddr + tB * c + PW * q, a4);
+          tm::wait_ld4(a4);
+          ar = tm::join(a4[0], a4[1]);
+          ai = tm::join(a4[2], a4[3]);
+        } else {
+          uint32_t a2[2];
+          tm::ld2(taddr + tB * c + PW * q, a2);
+          tm::wait_ld2(a2);
+          ar = (double)__uint_as_float(a2[0]);
+          ai = (double)__uint_as_float(a2[1]);
+        }
         double pr = 1.0, pi = 0.0;
         if (phase) {
           const double root = root_of(nA + c, m);
@@ -1543,24 +1599,25 @@ __host__ __device__ constexpr size_t cols_pair_smem_bytes() {
   return 2 * (size_t)(1 << LOGN) * sizeof(typename V2<T>::t) + 16;
 }
 
-// TMEM columns a pair block of G threads allocates: 128 per warp of a lane
-// quarter (16 pixels x 8 words).
-__host__ __device__ constexpr uint32_t pair_tm_cols(int threads) {
-  return (uint32_t)(threads / 32 / 4) * 128u;
+// TMEM columns a pair block of `threads` threads allocates: 16 pixels x W
+// words per warp of a lane quarter.
+template <typename T> __host__ __device__ constexpr uint32_t pair_tm_cols(int threads) {
+  return (uint32_t)(threads / 32 / 4) * 16u * pair_pixel_words<T>();
 }
 
 // One job's column pass, column pairs (nx / 2 of them) over a persistent grid.
-// Blocks of G threads, 512 / G of them per SM (the TMEM they allocate): at most
-// 128 registers a thread.
-template <int LOGN> constexpr int pair_min_blocks() {
-  return (int)(512u / pair_tm_cols(group_threads<LOGN>()));
+// Blocks of G threads, as many per SM as their TMEM allows (512 / the columns
+// a block allocates): 128 registers a thread for the FP64 pass, 64 for the
+// FP32 pass (twice the blocks).
+template <typename T, int LOGN> constexpr int pair_min_blocks() {
+  return (int)(512u / pair_tm_cols<T>(group_threads<LOGN>()));
 }
 
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>())
+__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<T, LOGN>())
     k_fft_cols_pair(ColJob<T> J) {
   constexpr int N = 1 << LOGN;
-  constexpr uint32_t ncols = pair_tm_cols(group_threads<LOGN>());
+  constexpr uint32_t ncols = pair_tm_cols<T>(group_threads<LOGN>());
   using V = typename V2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *sA = reinterpret_cast<V *>(smem_raw);
@@ -1575,7 +1632,8 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>()
   __syncthreads();
   tm::fence_after();
   const uint32_t tbase = *slot;
-  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 128u;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) +
+                         (uint32_t)(warp / 4) * 16u * pair_pixel_words<T>();
   const uint32_t pairs = (uint32_t)J.nx / 2u;
   for (uint32_t p = blockIdx.x; p < pairs; p += gridDim.x) {
     fft_col_pair_tm<T, LOGN>(sA, sB, 2u * p, J, taddr);
@@ -1594,12 +1652,12 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>()
 // col_units[k]*rpc .. col_units[k+1]*rpc - 1 (each job's count even), taken
 // two at a time.
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>())
+__global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<T, LOGN>())
     k_fft_cols_pair_multi(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ col_jobs,
                           int lo, int hi, const uint32_t *__restrict__ col_units, int rpc,
                           const uint32_t *__restrict__ rowmask, const uint32_t *__restrict__ counts) {
   constexpr int N = 1 << LOGN;
-  constexpr uint32_t ncols = pair_tm_cols(group_threads<LOGN>());
+  constexpr uint32_t ncols = pair_tm_cols<T>(group_threads<LOGN>());
   using V = typename V2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *sA = reinterpret_cast<V *>(smem_raw);
@@ -1614,33 +1672,42 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<LOGN>()
   __syncthreads();
   tm::fence_after();
   const uint32_t tbase = *slot;
-  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * 128u;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) +
+                         (uint32_t)(warp / 4) * 16u * pair_pixel_words<T>();
   const uint32_t p0 = col_units[lo] * (uint32_t)rpc / 2u, p1 = col_units[hi] * (uint32_t)rpc / 2u;
+  // the pair's job, in shared memory (its fields are read where used, not held
+  // in registers across the transform)
+  __shared__ ColJob<T> sJ;
+  __shared__ uint32_t sA0;
   for (uint32_t p = p0 + blockIdx.x; p < p1; p += gridDim.x) {
-    const int k = lo + batch_job_of(col_units + lo, hi - lo, 2u * p / (uint32_t)rpc);
-    const BatchJob &B = jobs[col_jobs[k]];
-    ColJob<T> J;
-    J.cube = (const V *)B.blocked;
-    J.nx = B.g.nx;
-    J.ny = B.g.ny;
-    J.nw = B.g.nw;
-    J.nty = B.g.nty;
-    J.w_first = B.g.w_first;
-    J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
-    J.rowmask = rowmask + B.mask_base;
-    J.counts = counts + B.counts_base;
-    J.tw = (const V *)B.tw_y;
-    J.ltab = B.ltab;
-    J.mtab = B.mtab;
-    J.wmin = B.wmin;
-    J.dw = B.dw_phase;
-    J.dwnorm = B.dwnorm;
-    J.norm = B.norm;
-    J.phase_on = B.phase_on;
-    J.img_re = B.img_re;
-    J.img_im = B.img_im;
-    fft_col_pair_tm<T, LOGN>(sA, sB, 2u * p - col_units[k] * (uint32_t)rpc, J, taddr);
+    if (threadIdx.x == 0) {
+      const int k = lo + batch_job_of(col_units + lo, hi - lo, 2u * p / (uint32_t)rpc);
+      const BatchJob &B = jobs[col_jobs[k]];
+      ColJob<T> &J = sJ;
+      sA0 = 2u * p - col_units[k] * (uint32_t)rpc;
+      J.cube = (const V *)B.blocked;
+      J.nx = B.g.nx;
+      J.ny = B.g.ny;
+      J.nw = B.g.nw;
+      J.nty = B.g.nty;
+      J.w_first = B.g.w_first;
+      J.nw_total = B.g.nw_total > 0 ? B.g.nw_total : B.g.nw;
+      J.rowmask = rowmask + B.mask_base;
+      J.counts = counts + B.counts_base;
+      J.tw = (const V *)B.tw_y;
+      J.ltab = B.ltab;
+      J.mtab = B.mtab;
+      J.wmin = B.wmin;
+      J.dw = B.dw_phase;
+      J.dwnorm = B.dwnorm;
+      J.norm = B.norm;
+      J.phase_on = B.phase_on;
+      J.img_re = B.img_re;
+      J.img_im = B.img_im;
+    }
     __syncthreads();
+    fft_col_pair_tm<T, LOGN>(sA, sB, sA0, sJ, taddr);
+    __syncthreads();  // the buffers and the job are rewritten for the next pair
   }
   tm::fence_before();
   __syncthreads();
@@ -1932,7 +1999,7 @@ bool cols_pair_enabled() {
 template <typename T, int LOGN>
 int launch_cols_pair(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int BT = group_threads<LOGN>();
-  const int max_blocks = (int)(512u / pair_tm_cols(BT));
+  const int max_blocks = (int)(512u / pair_tm_cols<T>(BT));
   int dev = 0, smem_sm = 0, reserved = 0;
   RICK_CUDA(cudaGetDevice(&dev));
   RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
