@@ -1225,17 +1225,18 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
 // pass apart: in each barrier interval it computes one pass of one column on
 // values already in registers while it loads the inputs of the other column's
 // next pass, so both pipes are busy at once.  Per plane (N = 1024..4096: a
-// first pass, two middle passes, a last pass of radix N/512 to registers) the
-// intervals are
+// first pass, two radix-8 middle passes, a last pass of radix N/512 to
+// registers; N = 8192, FP32 only: three middle passes and a radix-2 last
+// pass) the intervals are
 //   A: read rows | first pass | read | pass 2 | read | pass 3 | read | last + w-step
 //   B: last + w-step (previous plane) | read rows | first pass | read | ... | read
-// with a barrier after each interval from the second to the seventh (the
+// with a barrier after each interval from the second to the last but one (the
 // first two and the last touch no shared memory the other threads use next).
 // The first pass's inputs (the plane's touched rows) come from the cube
 // straight into registers; the next plane's rows are prefetched into L2 a
 // plane ahead.  Each thread holds 16 pixels' running sums and w-steps in TMEM
-// (8 of each column): a block of N/8 threads allocates N/8 TMEM columns, all
-// 512 of its SM at N = 4096.
+// (8 of each column): a block of N/8 threads allocates N/8 TMEM columns with
+// FP64 state (all 512 of its SM at N = 4096), N/16 with FP32 state.
 
 __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
@@ -1411,8 +1412,11 @@ __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], 
 template <typename T, int LOGN>
 __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename V2<T>::t *sB,
                                                 uint32_t nA, const ColJob<T> &J, uint32_t taddr) {
-  static_assert(LOGN >= 10 && LOGN <= 12, "the pair schedule is written for four passes");
-  constexpr int N = 1 << LOGN, G = N / kVpt, LASTR = N / 512;
+  static_assert(LOGN >= 10 && LOGN <= 13, "the pair schedule has two or three middle passes");
+  constexpr int N = 1 << LOGN, G = N / kVpt;
+  constexpr int NMID = LOGN <= 12 ? 2 : 3;              // radix-8 passes after the first
+  constexpr int NSL = NMID == 2 ? 512 : 4096;           // stride of the last pass
+  constexpr int LASTR = N / NSL;                        // its radix (2, 4 or 8)
   constexpr int CB = col_block<T>();
   using V = typename V2<T>::t;
   const int t = threadIdx.x;
@@ -1465,9 +1469,8 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
   // the per-pixel steps into TMEM
   const double dwstep = __dmul_rn(twopi, J.dw);
   // the thread's twiddle entries, formed where used (fewer live registers)
-  auto tw1 = [&] { return J.tw + 7 + (t & 7); };
-  auto tw2 = [&] { return J.tw + 63 + (t & 63); };
-  auto twl = [&] { return J.tw + (N / LASTR - 1) + t; };
+  auto tw_mid = [&](int Ns) { return J.tw + (Ns - 1) + (t & (Ns - 1)); };
+  auto twl = [&] { return J.tw + (NSL - 1) + t; };
   constexpr uint32_t PW = pair_pixel_words<T>(), tB = 8 * PW;  // column B's TMEM offset
 #pragma unroll
   for (int c = 0; c < 2; c++) {
@@ -1510,22 +1513,17 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     pair_read<T, N>(sA, t, vA);
     pair_first<T>(sB, t, vB);
     __syncthreads();
-    // A: pass 2 | B: read
-    pair_read<T, N>(sB, t, vB);
-    pair_mid<T>(sA, t, 8, __ldg(tw1()), vA);
-    __syncthreads();
-    // A: read | B: pass 2
-    pair_read<T, N>(sA, t, vA);
-    pair_mid<T>(sB, t, 8, __ldg(tw1()), vB);
-    __syncthreads();
-    // A: pass 3 | B: read
-    pair_read<T, N>(sB, t, vB);
-    pair_mid<T>(sA, t, 64, __ldg(tw2()), vA);
-    __syncthreads();
-    // A: read | B: pass 3
-    pair_read<T, N>(sA, t, vA);
-    pair_mid<T>(sB, t, 64, __ldg(tw2()), vB);
-    __syncthreads();
+    // the middle passes, of strides 8, 64 (, 512): A computes while B reads,
+    // then A reads while B computes
+#pragma unroll
+    for (int mp = 0, Ns = 8; mp < NMID; mp++, Ns *= 8) {
+      pair_read<T, N>(sB, t, vB);
+      pair_mid<T>(sA, t, Ns, __ldg(tw_mid(Ns)), vA);
+      __syncthreads();
+      pair_read<T, N>(sA, t, vA);
+      pair_mid<T>(sB, t, Ns, __ldg(tw_mid(Ns)), vB);
+      __syncthreads();
+    }
     // A: last pass and w-step | B: read (its last pass runs with the next plane's rows)
     pair_read<T, N>(sB, t, vB);
     pair_last<T, LASTR>(twl(), G, vA);
@@ -1993,7 +1991,7 @@ bool cols_pair_enabled() {
 }
 
 // The two-column pass (one job, or the jobs of a batch class), for column
-// lengths 1024..4096.  A block of G threads allocates G TMEM columns; its
+// lengths 1024..4096 (and 8192 for one FP32 job).  A block of G threads allocates G TMEM columns; its
 // dynamic shared memory is padded so that shared memory, not the TMEM
 // allocation, bounds the blocks per SM (a further block could not allocate).
 template <typename T, int LOGN>
@@ -2047,10 +2045,11 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr size_t kMax = 220 * 1024;
   // the TMEM-state passes: always for one job; for a batch when its schedule
   // asks for them (planes in flight 0).  Two columns per block from 1024 to
-  // 4096 points (both columns' buffers in shared memory), one below and above.
+  // 4096 points, and at 8192 for FP32 (both columns' buffers in shared
+  // memory), one column per block otherwise.
   const bool tm_one = cols_tm_enabled() && f.one;
   const bool tm_batch = cols_tm_enabled() && !f.one && f.cols_pp == 0 && LOGN <= kMultiMaxLog;
-  if constexpr (LOGN >= 10 && LOGN <= 12) {
+  if constexpr ((LOGN >= 10 && LOGN <= 12) || (LOGN == 13 && sizeof(T) == 4)) {
     if ((tm_one || tm_batch) && cols_pair_enabled()) return launch_cols_pair<T, LOGN>(f, c, st);
   }
   if (tm_one) return launch_cols_tm<T, LOGN>(f, c, st);
