@@ -367,7 +367,7 @@ int rick_kernel_names(const char **names, int max_names) {
   static const char *k[] = {"k_bin_count",        "k_item_count",       "k_bin_scatter",
                             "k_scan_block",       "k_scan_add",         "k_grid_tiles",
                             "k_zero_split_tiles", "k_row_list",         "k_fft_units",
-                            "k_fft_rows",         "k_fft_cols_image",   "k_fft_cols_tm",      "k_fft_cols_tm_multi", "k_fft_cols_pair", "k_phase_sum",
+                            "k_fft_rows",         "k_fft_cols_image",   "k_fft_cols_tm",      "k_fft_cols_tm_multi", "k_fft_cols_pair", "k_fft_cols_pair_multi", "k_fft_cols_split", "k_phase_sum",
                             "k_export_cube",      "k_import_cube",      "k_bin_count_batch",
                             "k_bin_scatter_batch", "k_grid_tiles_batch", "k_zero_split_tiles_batch",
                             "k_fft_rows_multi",   "k_fft_cols_multi",   "k_uvw_init",

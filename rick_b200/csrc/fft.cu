@@ -1405,16 +1405,21 @@ __device__ __forceinline__ void pair_horner(uint32_t tcol, const Cx<T> (&x)[8], 
 }
 
 // Columns nA and nA + 1 (nA even) of one job; taddr is the thread's TMEM base
-// (column A's pixels at +0, column B's at +8W, W = pair_pixel_words).  The w1 twiddles of the
-// thread's butterflies are read where they are used (L1 hits).  For N =
-// 2^LOGN, LOGN = 10..12: a radix-8 first pass, two radix-8 middle passes
-// (strides 8 and 64), a last pass of radix N/512 (stride 512).
-template <typename T, int LOGN>
+// (A's pixels at +0, B's at +8W, W = pair_pixel_words).  The w1 twiddles of the
+// thread's butterflies are read where they are used (L1 hits).
+// SPLIT: one column nA of length 2N (8192), as two transforms of length N:
+// with x_lo = x[j], x_hi = x[j + N] (j < N), A transforms x_lo + x_hi (its
+// outputs are the column's even rows 2k) and B transforms
+// (x_lo - x_hi)·exp(+2 pi i j / 2N) (the odd rows 2k + 1) -- the first pass
+// of a decimation-in-frequency radix-2 step, done as the rows are read.
+template <typename T, int LOGN, bool SPLIT = false>
 __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename V2<T>::t *sB,
                                                 uint32_t nA, const ColJob<T> &J, uint32_t taddr) {
-  static_assert(LOGN >= 10 && LOGN <= 13, "the pair schedule has two or three middle passes");
-  constexpr int N = 1 << LOGN, G = N / kVpt;
-  constexpr int NMID = LOGN <= 12 ? 2 : 3;              // radix-8 passes after the first
+  constexpr int LF = SPLIT ? LOGN - 1 : LOGN;           // length of the transforms run
+  static_assert(LF >= 10 && LF <= 13, "the pair schedule has two or three middle passes");
+  static_assert(!SPLIT || LOGN == 13, "the split form is for 8192-point columns");
+  constexpr int N = 1 << LF, G = N / kVpt;
+  constexpr int NMID = LF <= 12 ? 2 : 3;                // radix-8 passes after the first
   constexpr int NSL = NMID == 2 ? 512 : 4096;           // stride of the last pass
   constexpr int LASTR = N / NSL;                        // its radix (2, 4 or 8)
   constexpr int CB = col_block<T>();
@@ -1428,12 +1433,13 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
     do { iw--; } while (iw >= 0 && counts[1 + iw] == 0);
     return iw;
   };
-  // bit q: whether row t + q*G of plane iw was touched (the same for A and B)
+  // bit q: whether row t + q*G of plane iw was touched (the same for A and B);
+  // SPLIT: bit 8 + q for row t + q*G + N
   auto row_bits = [&](int iw) {
     const uint32_t *__restrict__ mask = J.rowmask + (uint64_t)iw * nty;
     uint32_t bits = 0;
 #pragma unroll
-    for (int q = 0; q < kVpt; q++) {
+    for (int q = 0; q < (SPLIT ? 2 * kVpt : kVpt); q++) {
       const int k = t + q * G;
       bits |= ((__ldg(mask + (k >> 5)) >> (k & 31)) & 1u) << q;
     }
@@ -1451,13 +1457,43 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
       }
     }
   };
+  // SPLIT: transform c's inputs (A: c = 0, B: c = 1) from the rows t + q*G
+  // and t + q*G + N of plane iw (read twice, once for each: the second read
+  // hits the caches)
+  auto read_half = [&](int iw, uint32_t bits, int c, Cx<T>(&v)[8]) {
+    const V *col = J.cube + blocked_index<T>(iw, 0, nA, nx, ny);
+    typename V2<T>::t wt;
+    if (c) wt = __ldg(J.tw + (N - 1) + t);  // exp(+2 pi i t / 2N), the 2N-point table's last pass
+#pragma unroll
+    for (int q = 0; q < kVpt; q++) {
+      Cx<T> lo = {(T)0, (T)0}, hi = {(T)0, (T)0};
+      if ((bits >> q) & 1u) {
+        const V x = __ldg(col + (uint64_t)(t + q * G) * CB);
+        lo = {x.x, x.y};
+      }
+      if ((bits >> (kVpt + q)) & 1u) {
+        const V x = __ldg(col + (uint64_t)(t + q * G + N) * CB);
+        hi = {x.x, x.y};
+      }
+      if (c == 0) {
+        v[q] = cadd(lo, hi);
+      } else {
+        // exp(+2 pi i (t + q*G) / 2N) = exp(+2 pi i q / 16) * exp(+2 pi i t / 2N)
+        const Cx<T> d = w16<T>(csub(lo, hi), q);
+        v[q] = cmul<T>(d, wt.x, wt.y);
+      }
+    }
+  };
   // the same rows into L2 (one 32-byte sector holds both columns' values)
   auto prefetch_rows = [&](int iw, uint32_t bits) {
     const V *col = J.cube + blocked_index<T>(iw, 0, nA, nx, ny);
 #pragma unroll
-    for (int q = 0; q < kVpt; q++)
+    for (int q = 0; q < (SPLIT ? 2 * kVpt : kVpt); q++)
       if ((bits >> q) & 1u) prefetch_l2(col + (uint64_t)(t + q * G) * CB);
   };
+  // the pixel of transform c's value q: (column, row)
+  auto pix_col = [&](int c) { return SPLIT ? nA : nA + (uint32_t)c; };
+  auto pix_row = [&](int c, int q) { return SPLIT ? 2 * (t + q * G) + c : t + q * G; };
   // sqrt(1 - l^2 - m^2), phase_correction.cu:56-64
   auto root_of = [&](uint32_t n, int m) {
     const double l = J.ltab[n];
@@ -1476,9 +1512,9 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
   for (int c = 0; c < 2; c++) {
 #pragma unroll
     for (int q = 0; q < kVpt; q++) {
-      const int m = t + q * G;
       double sn = 0.0, cs = 1.0;
-      if (phase) sincos(__dmul_rn(dwstep, __dsub_rn(root_of(nA + c, m), 1.0)), &sn, &cs);
+      if (phase)
+        sincos(__dmul_rn(dwstep, __dsub_rn(root_of(pix_col(c), pix_row(c, q)), 1.0)), &sn, &cs);
       if constexpr (PW == 8) {
         uint32_t w4[4];
         tm::split(cs, w4[0], w4[1]);
@@ -1497,7 +1533,10 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
   int prev = iw, b_gap = 0;
   while (iw >= 0) {
     // A: the plane's rows | B: last pass and w-step of the previous plane
-    read_rows(iw, bits, nA, vA);
+    if constexpr (SPLIT)
+      read_half(iw, bits, 0, vA);
+    else
+      read_rows(iw, bits, nA, vA);
     const int nxt = prev_plane(iw);
     const uint32_t nbits = nxt >= 0 ? row_bits(nxt) : 0u;
     if (b_pending) {
@@ -1505,7 +1544,10 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
       pair_horner<T>(taddr + tB, vB, b_first, b_gap);
     }
     // A: first pass | B: the plane's rows
-    read_rows(iw, bits, nA + 1, vB);
+    if constexpr (SPLIT)
+      read_half(iw, bits, 1, vB);
+    else
+      read_rows(iw, bits, nA + 1, vB);
     pair_first<T>(sA, t, vA);
     if (nxt >= 0) prefetch_rows(nxt, nbits);
     __syncthreads();
@@ -1547,7 +1589,6 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
                     15u) == 0;
 #pragma unroll
   for (int q = 0; q < kVpt; q++) {
-    const int m = t + q * G;
     double re[2] = {0.0, 0.0}, im[2] = {0.0, 0.0};
     if (!first) {
 #pragma unroll
@@ -1568,7 +1609,7 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
         }
         double pr = 1.0, pi = 0.0;
         if (phase) {
-          const double root = root_of(nA + c, m);
+          const double root = root_of(pix_col(c), pix_row(c, q));
           double sn, cs;
           sincos(__dmul_rn(cw, __dsub_rn(root, 1.0)), &sn, &cs);
           const double amp = J.dwnorm * root;
@@ -1579,7 +1620,16 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
         im[c] = J.norm * fma(ar, pi, ai * pr);
       }
     }
-    const uint64_t o = (uint64_t)m * nx + nA;
+    if constexpr (SPLIT) {  // rows 2k and 2k + 1 of one column
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const uint64_t o = (uint64_t)pix_row(c, q) * nx + nA;
+        J.img_re[o] = re[c];
+        J.img_im[o] = im[c];
+      }
+      continue;
+    }
+    const uint64_t o = (uint64_t)(t + q * G) * nx + nA;
     if (vec) {
       *reinterpret_cast<double2 *>(J.img_re + o) = make_double2(re[0], re[1]);
       *reinterpret_cast<double2 *>(J.img_im + o) = make_double2(im[0], im[1]);
@@ -1636,6 +1686,42 @@ __global__ void __launch_bounds__(group_threads<LOGN>(), pair_min_blocks<T, LOGN
   for (uint32_t p = blockIdx.x; p < pairs; p += gridDim.x) {
     fft_col_pair_tm<T, LOGN>(sA, sB, 2u * p, J, taddr);
     __syncthreads();  // the column buffers are rewritten for the next pair
+  }
+  tm::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tm::fence_after();
+    tm::dealloc(tbase, ncols);
+  }
+}
+
+// One job's column pass at 8192 points with FP64 state: each column split into
+// two 4096-point transforms (even and odd rows) run one pass apart, columns
+// over a persistent grid of one block per SM.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(group_threads<LOGN - 1>(), 1) k_fft_cols_split(ColJob<T> J) {
+  constexpr int NH = 1 << (LOGN - 1);
+  constexpr uint32_t ncols = pair_tm_cols<T>(group_threads<LOGN - 1>());
+  using V = typename V2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *sA = reinterpret_cast<V *>(smem_raw);
+  V *sB = sA + NH;
+  uint32_t *slot =
+      reinterpret_cast<uint32_t *>(smem_raw + cols_pair_smem_bytes<T, LOGN - 1>() - 16);
+  const int warp = threadIdx.x / 32;
+  if (warp == 0) {
+    tm::alloc(slot, ncols);
+    tm::relinquish();
+  }
+  tm::fence_before();
+  __syncthreads();
+  tm::fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp % 4)) << 16) +
+                         (uint32_t)(warp / 4) * 16u * pair_pixel_words<T>();
+  for (uint32_t n = blockIdx.x; n < (uint32_t)J.nx; n += gridDim.x) {
+    fft_col_pair_tm<T, LOGN, true>(sA, sB, n, J, taddr);
+    __syncthreads();  // the buffers are rewritten for the next column
   }
   tm::fence_before();
   __syncthreads();
@@ -2036,6 +2122,31 @@ int launch_cols_pair(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   return RICK_OK;
 }
 
+// The split pass (one FP64 job, 8192-point columns): one block per SM, which
+// allocates all 512 TMEM columns; shared memory padded above half the SM's.
+template <typename T, int LOGN>
+int launch_cols_split(const BatchJob &B, const FftJobs &f, cudaStream_t st) {
+  constexpr int BT = group_threads<LOGN - 1>();
+  int dev = 0, smem_sm = 0, reserved = 0;
+  RICK_CUDA(cudaGetDevice(&dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RICK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  size_t sm = cols_pair_smem_bytes<T, LOGN - 1>();
+  const size_t floor_b = (size_t)smem_sm / 2 + 1;
+  if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
+  sm = (sm + 15) & ~(size_t)15;
+  const void *fn = (const void *)k_fft_cols_split<T, LOGN>;
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int pct = (int)std::min<size_t>(
+      100, ((sm + (size_t)reserved) * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+  RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  const int blocks = std::max(1, std::min(B.g.nx, num_sms()));
+  RICK_LAUNCHED();
+  k_fft_cols_split<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(B, f));
+  RICK_CUDA(cudaGetLastError());
+  return RICK_OK;
+}
+
 template <typename T, int LOGN>
 int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   constexpr int G = group_threads<LOGN>(), BT = block_threads<LOGN>();
@@ -2046,11 +2157,15 @@ int launch_cols(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   // the TMEM-state passes: always for one job; for a batch when its schedule
   // asks for them (planes in flight 0).  Two columns per block from 1024 to
   // 4096 points, and at 8192 for FP32 (both columns' buffers in shared
-  // memory), one column per block otherwise.
+  // memory); at 8192 for FP64 one column split into two 4096-point halves;
+  // one column per block otherwise.
   const bool tm_one = cols_tm_enabled() && f.one;
   const bool tm_batch = cols_tm_enabled() && !f.one && f.cols_pp == 0 && LOGN <= kMultiMaxLog;
   if constexpr ((LOGN >= 10 && LOGN <= 12) || (LOGN == 13 && sizeof(T) == 4)) {
     if ((tm_one || tm_batch) && cols_pair_enabled()) return launch_cols_pair<T, LOGN>(f, c, st);
+  }
+  if constexpr (LOGN == 13 && sizeof(T) == 8) {
+    if (tm_one && cols_pair_enabled()) return launch_cols_split<T, LOGN>(*f.one, f, st);
   }
   if (tm_one) return launch_cols_tm<T, LOGN>(f, c, st);
   if constexpr (LOGN <= kMultiMaxLog) {
