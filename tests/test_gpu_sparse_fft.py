@@ -163,10 +163,13 @@ def _pair_case_rows(seed, n, nw, planes=None):
     (64, 1024, 6, False, None),                 # 1024-point columns (radix-2), phase off
     (256, 1024, 16, True, [1, 2, 5, 13, 14]),   # planes without rows between planes with rows
     (64, 4096, 7, True, [0, 6]),                # the first and last planes only
+    (64, 8192, 6, True, [0, 3, 5]),             # 8192 points: FP64 split in halves, FP32 pairs
+    (128, 8192, 3, False, None),                # 8192 points, PHASE_ON off
 ])
 def test_two_column_pass_vs_oracle(nx, ny, nw, phase_on, planes):
-    """Column lengths 1024..4096 run two columns per block, one pass apart:
-    each form against the oracle, including plane gaps and PHASE_ON off."""
+    """Column lengths 1024..8192 run two transforms per block, one pass apart
+    (at 8192 FP64, the even and odd rows of one column): each form against the
+    oracle, including plane gaps and PHASE_ON off."""
     n = 5000
     host = _pair_case_rows(nx + ny + nw, n, nw, planes)
     rows = gpu_rows(*host)
