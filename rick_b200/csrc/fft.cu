@@ -1484,7 +1484,8 @@ __device__ __forceinline__ void fft_col_pair_tm(typename V2<T>::t *sA, typename 
       }
     }
   };
-  // the same rows into L2 (one 32-byte sector holds both columns' values)
+  // the same rows into L2 (pairs: one 32-byte sector holds both columns'
+  // values; SPLIT: both halves of the column)
   auto prefetch_rows = [&](int iw, uint32_t bits) {
     const V *col = J.cube + blocked_index<T>(iw, 0, nA, nx, ny);
 #pragma unroll
