@@ -142,6 +142,11 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
 }
 
+// A global address's line into L2 (no register is written).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 constexpr int kVpt = 8;  // values per thread
 
 // Row-transformed planes are stored column-blocked: 128-byte blocks of
@@ -492,6 +497,24 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), row_min_blocks<LOGN>())
     const uint32_t li = base + grp;
     const bool active = li < nrows;
     const uint32_t rid = active ? rowlist[li] : 0;
+    if constexpr (LOGN >= 13) {
+      // 8192-point rows: one block (one row) per SM, so the next row's touched
+      // tiles are prefetched into L2 while this one is transformed (c3 row pass
+      // 5.51 -> 5.14 ms FP64; at 4096 points, two blocks per SM, it slowed it)
+      const uint32_t ln = li + gridDim.x * rpc;
+      if (ln < nrows) {
+        const uint32_t rn = rowlist[ln];
+        const uint32_t wn = rn / (uint32_t)ny, kn = rn % (uint32_t)ny;
+        const uint32_t *tmn = tilemask + ((uint64_t)wn * nty + (kn >> 5)) * tmw;
+        const typename V2<T>::t *pn = cube + ((uint64_t)wn * ny + kn) * nx;
+        const int t = threadIdx.x % G;
+#pragma unroll
+        for (int q = 0; q < kVpt; q++) {
+          const int x = t + q * G;
+          if ((tmn[x >> 10] >> ((x >> 5) & 31)) & 1u) prefetch_l2(pn + x);
+        }
+      }
+    }
     fft_row_unit<T, LOGN>(s, active, rid / (uint32_t)ny, rid % (uint32_t)ny, cube, out, nx, ny,
                           nty, tmw, tilemask, tw);
   }
@@ -1237,10 +1260,6 @@ __global__ void __launch_bounds__(block_threads<LOGN>(), tm_min_blocks<LOGN>())
 // plane ahead.  Each thread holds 16 pixels' running sums and w-steps in TMEM
 // (8 of each column): a block of N/8 threads allocates N/8 TMEM columns with
 // FP64 state (all 512 of its SM at N = 4096), N/16 with FP32 state.
-
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
-}
 
 // v[r] *= w1^r (r = 1..7), the powers formed from w1 as in pass_twiddles.
 template <typename T>
