@@ -124,8 +124,10 @@ __device__ __forceinline__ double item_scale(const RecF64 *__restrict__ rec, uin
 
 // Records r0..r1 of tile (tx, ty) of plane w: footprints accumulated in the
 // shared tile (s_re, s_im, zeroed by the caller), then the tile written to the
-// cube and the rows/tile it touched marked.  LPR lanes per record (a power of
-// two >= w_support); 32/LPR records per warp step.
+// cube and the rows/tile it touched marked.  LPR lanes per record (>= w_support:
+// 8 or 16, or the support itself when it is a compile-time constant that does
+// not divide 32 well -- 9 lanes give three records a warp step where 16 gave
+// two); 32/LPR records per warp step, lanes past RPW*LPR idle.
 template <typename OutT, int LPR, int SUP = 0>
 __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32_t r0, uint32_t r1,
                                           const Geometry &g, bool hi, const double *s_tab,
@@ -149,7 +151,7 @@ __device__ __forceinline__ void grid_item(const RecF64 *__restrict__ rec, uint32
   // Footprints of the chunk's records into the shared tile.
   for (uint32_t rb = r0 + (warp * RPW); rb < r1; rb += kWarps * RPW) {
     const uint32_t r = rb + lane / LPR;
-    const bool valid = r < r1;
+    const bool valid = lane < (unsigned)(RPW * LPR) && r < r1;
     RecF64 q;
     if (valid) q = rec[r];
     else q.sre = q.sim = q.pu = q.pv = 0.0;
@@ -429,11 +431,12 @@ int launch_grid(const Geometry &g, int kernel, Scratch &s, void *cube, int accum
   k_grid_tiles<OutT, LPR, SUP><<<blocks, kGridThreads, 0, st>>>(                               \
       s.records, s.bin_count, s.item_off, nbins, max_chunk, g, kernel, s.table, accumulate,    \
       s.counters, (V *)cube, rowmask, tilemask)
-  // the common supports unrolled (7: 1.16 -> 1.00 ms FP64 at 4096^2 x 32)
+  // the common supports unrolled (7: 1.16 -> 1.00 ms FP64 at 4096^2 x 32; 9
+  // with 9 lanes a record: 1.73 -> 1.20 ms at 8192^2 x 64)
   if (g.support == 7)
     RICK_GRID(8, 7);
   else if (g.support == 9)
-    RICK_GRID(16, 9);
+    RICK_GRID(9, 9);
   else if (g.support <= 8)
     RICK_GRID(8, 0);
   else
@@ -490,7 +493,7 @@ int launch_grid_batch(const BatchLaunch &b, Scratch &s, uint32_t max_chunk, cuda
   if (b.min_support == 7 && b.max_support == 7)
     RICK_GRID(8, 7);
   else if (b.min_support == 9 && b.max_support == 9)
-    RICK_GRID(16, 9);
+    RICK_GRID(9, 9);
   else if (b.max_support <= 8)
     RICK_GRID(8, 0);
   else
