@@ -169,6 +169,13 @@ struct rick_batch {
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   uint32_t kernels_per_run = 0;  // kernel nodes of the captured graph
+  // Batches launched side by side on several streams (the server): the column
+  // pass waits for this event and records it, so that the column passes of two
+  // batches never run at once.  Their blocks allocate tensor memory, and blocks
+  // of two such kernels may share an SM by shared memory and registers yet ask
+  // for more than its 512 TMEM columns together; a block that cannot allocate
+  // waits, holding its SM.  Null: no gate.
+  cudaEvent_t cols_gate = nullptr;
 };
 
 namespace {
@@ -184,7 +191,9 @@ int batch_launch(rick_batch *b, cudaStream_t st) {
   RICK_TRY(grid_tiles_batch(b->bl, b->precision, b->s, b->tune.max_chunk, st));
   RICK_TRY(sparse_fft_lists(b->fj, st));
   RICK_TRY(sparse_fft_rows(b->fj, b->precision, st));
+  if (b->cols_gate) RICK_CUDA(cudaStreamWaitEvent(st, b->cols_gate, 0));
   RICK_TRY(sparse_fft_cols(b->fj, b->precision, st));
+  if (b->cols_gate) RICK_CUDA(cudaEventRecord(b->cols_gate, st));
   return RICK_OK;
 }
 
@@ -627,10 +636,11 @@ namespace rick {
 
 int batch_create_in(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
                     int device, void *arena, uint64_t arena_bytes, const rick_batch_tuning &t,
-                    cudaStream_t st) {
+                    cudaStream_t st, cudaEvent_t cols_gate) {
   RICK_TRY(batch_prepare(out, jobs, njobs, precision, device, arena, arena_bytes, st));
   (*out)->tune = t;
   (*out)->use_graph = false;
+  (*out)->cols_gate = cols_gate;
   return RICK_OK;
 }
 

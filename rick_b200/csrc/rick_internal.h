@@ -264,9 +264,11 @@ int sparse_fft_rows(const FftJobs &f, int precision, cudaStream_t st);
 int sparse_fft_cols(const FftJobs &f, int precision, cudaStream_t st);
 
 // The batch internals the serving loop (serve.cu) builds on (batch.cu).
+// cols_gate: an event the batch's column pass waits for and records (batches
+// launched side by side on several streams), or null.
 int batch_create_in(rick_batch **out, const rick_job_desc *jobs, int njobs, int precision,
                     int device, void *arena, uint64_t arena_bytes, const rick_batch_tuning &t,
-                    cudaStream_t st);
+                    cudaStream_t st, cudaEvent_t cols_gate);
 int batch_launch_eager(rick_batch *b, cudaStream_t st);
 void batch_destroy(rick_batch *b);
 uint64_t batch_bytes(const rick_job_desc *jobs, int njobs, int precision);

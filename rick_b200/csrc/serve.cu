@@ -70,6 +70,10 @@ struct rick_server {
   uint64_t used = 0;
   bool stop = false;
   std::thread th;
+  // the column passes of batches on different streams run one at a time (their
+  // blocks allocate tensor memory; see rick_batch::cols_gate); batches are
+  // launched by the scheduler thread alone, in order
+  cudaEvent_t cols_gate = nullptr;
   rick_batch_tuning tune{2048, 6, 1};
   rick_server_stats stats{};
 };
@@ -102,7 +106,7 @@ int launch_batch(rick_server *s, InFlight *f, const std::vector<rick_job_desc> &
   RICK_CUDA(cudaMallocFromPoolAsync(&arena, f->bytes, s->pool, st));
   rick_batch *b = nullptr;
   int r = batch_create_in(&b, descs.data(), (int)descs.size(), s->d.precision, s->d.device, arena,
-                          f->bytes, s->tune, st);
+                          f->bytes, s->tune, st, s->cols_gate);
   if (r == RICK_OK) r = batch_launch_eager(b, st);
   // stream-ordered: the arena returns to the pool once the batch has run
   const cudaError_t e = cudaFreeAsync(arena, st);
@@ -258,6 +262,7 @@ int rick_server_create(rick_server **out, const rick_server_desc *d) {
     uint64_t keep = d->hbm_budget;  // keep freed blocks for the next batches
     e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->cols_gate, cudaEventDisableTiming);
   for (int k = 0; k < d->streams && e == cudaSuccess; k++) {
     cudaStream_t st = nullptr;
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -275,6 +280,7 @@ int rick_server_create(rick_server **out, const rick_server_desc *d) {
     if (e == cudaErrorMemoryAllocation) {
       cudaGetLastError();
       for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+      if (s->cols_gate) cudaEventDestroy(s->cols_gate);
       cudaMemPoolDestroy(s->pool);
       delete s;
       return set_error(RICK_ERR_NOT_ENOUGH_MEM, "the device cannot hold a budget of %llu bytes",
@@ -284,6 +290,7 @@ int rick_server_create(rick_server **out, const rick_server_desc *d) {
   if (e != cudaSuccess) {
     const int r = cuda_status(e, "rick_server_create", __FILE__, __LINE__);
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    if (s->cols_gate) cudaEventDestroy(s->cols_gate);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return r;
@@ -393,6 +400,7 @@ int rick_server_destroy(rick_server *s) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
+  if (s->cols_gate) cudaEventDestroy(s->cols_gate);
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   return RICK_OK;
