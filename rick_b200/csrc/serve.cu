@@ -122,13 +122,31 @@ int launch_batch(rick_server *s, InFlight *f, const std::vector<rick_job_desc> &
 void scheduler(rick_server *s) {
   cudaSetDevice(s->d.device);
   std::unique_lock<std::mutex> lk(s->mu);
+  std::vector<InFlight *> running;
+  std::vector<cudaError_t> state;
   for (;;) {
-    // retire finished batches; a stream that reports an error will never run
-    // the completion function, so its jobs fail here
+    // A stream that reports an error will never run its completion function,
+    // so its jobs fail here.  The streams are queried without holding the
+    // lock: the completion function (run by CUDA's callback thread) takes it,
+    // and a CUDA call made while holding it could wait on that function.  Only
+    // this thread removes batches, so the pointers stay valid meanwhile.
+    running.clear();
+    for (InFlight *f : s->inflight)
+      if (!f->done) running.push_back(f);
+    state.assign(running.size(), cudaSuccess);
+    if (!running.empty()) {
+      lk.unlock();
+      for (size_t i = 0; i < running.size(); i++)
+        state[i] = cudaStreamQuery(s->streams[running[i]->stream]);
+      lk.lock();
+    }
+    // retire finished batches and those whose stream failed
     for (auto it = s->inflight.begin(); it != s->inflight.end();) {
       InFlight *f = *it;
       if (!f->done) {
-        const cudaError_t q = cudaStreamQuery(s->streams[f->stream]);
+        cudaError_t q = cudaSuccess;
+        for (size_t i = 0; i < running.size(); i++)
+          if (running[i] == f) q = state[i];
         if (q == cudaSuccess || q == cudaErrorNotReady) {
           ++it;
           continue;
