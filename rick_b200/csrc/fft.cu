@@ -2112,8 +2112,13 @@ int launch_cols_pair(const FftJobs &f, const FftClass &c, cudaStream_t st) {
   const size_t floor_b = (size_t)smem_sm / (size_t)(max_blocks + 1) + 1;
   if (sm + (size_t)reserved < floor_b) sm = floor_b - (size_t)reserved;
   sm = (sm + 15) & ~(size_t)15;
-  const void *fn = f.one ? (const void *)k_fft_cols_pair<T, LOGN>
-                         : (const void *)k_fft_cols_pair_multi<T, LOGN>;
+  // batches carry column lengths up to 2^kMultiMaxLog: no multi-job kernel beyond
+  const void *fn = (const void *)k_fft_cols_pair<T, LOGN>;
+  if constexpr (LOGN <= kMultiMaxLog) {
+    if (!f.one) fn = (const void *)k_fft_cols_pair_multi<T, LOGN>;
+  } else {
+    if (!f.one) return set_error(RICK_ERR_INVALID_ARG, "batch FFT length above %d", 1 << kMultiMaxLog);
+  }
   RICK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   cudaFuncAttributes fa{};
   RICK_CUDA(cudaFuncGetAttributes(&fa, fn));
@@ -2131,7 +2136,7 @@ int launch_cols_pair(const FftJobs &f, const FftClass &c, cudaStream_t st) {
     const BatchJob &B = *f.one;
     const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)B.g.nx / 2, slots));
     k_fft_cols_pair<T, LOGN><<<blocks, BT, sm, st>>>(col_job<T>(B, f));
-  } else {
+  } else if constexpr (LOGN <= kMultiMaxLog) {
     const int rpc = fft_rows_per_block(LOGN);
     const uint64_t pairs = (uint64_t)c.units * (uint64_t)rpc / 2u;
     const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(pairs, slots));
